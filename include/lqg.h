@@ -1,0 +1,170 @@
+/* liteqg_b200 — C ABI of the B200 quantized-graph query path.
+ *
+ * A drop-in for the query path of LiteQG's symphonyqg.Index (a SymphonyQG
+ * fork): the same index file, the same search semantics, bit-exact ids, on one
+ * NVIDIA B200 (sm_100a). Plain pointers and sizes only; every call returns an
+ * lqg_status and never throws. Host buffers belong to the caller, device
+ * buffers to the library. One lqg_index may be used from one host thread at a
+ * time; distinct indexes may be used concurrently on distinct streams.
+ *
+ * Reference interfaces replaced (paths inside the LiteQG project):
+ *   python/bindings.cpp:38-61   Index(index_type, metric, num_elements, dimension, degree_bound)
+ *   python/bindings.cpp:63,65   Index.load / Index.save
+ *   python/bindings.cpp:67      Index.set_ef
+ *   python/bindings.cpp:69-90   Index.build_index
+ *   python/bindings.cpp:92-98   Index.search(query, k)
+ *   symqglib/qg/qg.hpp:206-243  QuantizedGraph::save_index/load_index/set_ef/search
+ *   symqglib/qg/qg.hpp:298-344  QuantizedGraph::search_qg_with_heap
+ */
+#ifndef LQG_H
+#define LQG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define LQG_API __attribute__((visibility("default")))
+#else
+#define LQG_API
+#endif
+
+typedef struct lqg_index lqg_index;
+
+typedef enum {
+    LQG_OK = 0,
+    LQG_ERR_ARG = 1,      /* bad argument (shape, metric, degree, k, ef ...) */
+    LQG_ERR_IO = 2,       /* file missing, short, or of the wrong size */
+    LQG_ERR_CUDA = 3,     /* a CUDA runtime call failed */
+    LQG_ERR_NOMEM = 4,    /* device or host allocation failed */
+    LQG_ERR_STATE = 5,    /* call made in the wrong state (no data, ef unset) */
+    LQG_ERR_CAPACITY = 6, /* a per-query work area overflowed; see lqg_last_error */
+    LQG_ERR_CORRUPT = 7   /* index content invalid (neighbour id out of range) */
+} lqg_status;
+
+#define LQG_NO_ID 0xFFFFFFFFu /* output slot the reference leaves unwritten */
+
+/* Text of the last error on this host thread ("" if none). */
+LQG_API const char* lqg_last_error(void);
+
+/* Index(index_type, metric, num_elements, dimension, degree_bound):
+ * python/bindings.cpp:38-61. index_type must be "QG", metric "L2",
+ * degree_bound a positive multiple of 32 (32 or 64 run on the GPU), and
+ * dimension in [33, 2048] (the reference's rotator aborts outside it,
+ * symqglib/utils/rotator.hpp:55-76). device: CUDA ordinal. */
+LQG_API lqg_status lqg_create(const char* index_type, const char* metric,
+                      uint64_t num_elements, uint32_t dimension,
+                      uint32_t degree_bound, int device, lqg_index** out);
+
+/* Frees everything the index owns. NULL is accepted. */
+LQG_API void lqg_free(lqg_index* ix);
+
+/* Index.load: symqglib/qg/qg.hpp:217-224. The file must be exactly
+ * 4 + 4*N*(D+deg) + N*D + 8*D bytes; every neighbour id must be < N.
+ * Uploads the neighbour lists, codes and SQ8 parameters to the device. */
+LQG_API lqg_status lqg_load(lqg_index* ix, const char* path);
+
+/* Index.save: symqglib/qg/qg.hpp:206-215 (same bytes). */
+LQG_API lqg_status lqg_save(const lqg_index* ix, const char* path);
+
+/* Sets the index content from host arrays (the file's fields):
+ * vectors[N][D] f32 (stored, not searched), nbrs[N][deg] u32,
+ * codes[N][D] u8, params[D][2] f32 (min, scale). Validates and uploads. */
+LQG_API lqg_status lqg_set_arrays(lqg_index* ix, uint32_t entry, const float* vectors,
+                          const uint32_t* nbrs, const uint8_t* codes,
+                          const float* params);
+
+/* Copies the index content out (any pointer may be NULL). */
+LQG_API lqg_status lqg_get_arrays(const lqg_index* ix, uint32_t* entry, float* vectors,
+                          uint32_t* nbrs, uint8_t* codes, float* params);
+
+/* Index.set_ef: symqglib/qg/qg.hpp:226-230. ef in [1, 512]. */
+LQG_API lqg_status lqg_set_ef(lqg_index* ix, uint32_t ef);
+
+/* Index.search(query, k): python/bindings.cpp:92-98 -> qg.hpp:235-243.
+ * One query, host buffers, synchronous; the plain one-query-per-launch form.
+ * results[k] receives exactly the ids the reference writes (its worst-k of
+ * the ef pool in ascending distance, qg.hpp:340-343); slots it would leave
+ * unwritten (pool smaller than k) are LQG_NO_ID. */
+LQG_API lqg_status lqg_search(lqg_index* ix, const float* query, uint32_t k,
+                      uint32_t* results);
+
+/* Batched search (no reference counterpart; M > 1 form of Index.search).
+ * All pointers are DEVICE pointers; the call is asynchronous on `stream`
+ * (a cudaStream_t, NULL = legacy default stream).
+ *   queries  [m][D] f32
+ *   k, ef    per-query arrays [m] (u32) or NULL, then k0/ef0 apply to all
+ *            (ef0 == 0 means the value given to lqg_set_ef). With a per-query
+ *            ef array, ef0 must be an upper bound of its values (it sizes the
+ *            kernel's pool); per-query k values above kstride are clamped.
+ *   ids      [m][kstride] u32, compat output as lqg_search writes it
+ *   pool_ids [m][pstride] u32, pool_d [m][pstride] f32: the full final pool
+ *            in ascending distance (NULL to skip); unused slots LQG_NO_ID/inf
+ *   stats    [m][4] u32 (NULL to skip): pops, distance computations,
+ *            exact-path flag, pool size
+ * Queries whose pool meets two equal distances are re-run by the exact
+ * kernel (libstdc++ heap order) inside the same call, so ids always equal the
+ * reference's. */
+LQG_API lqg_status lqg_search_batch_device(lqg_index* ix, const float* queries,
+                                   int64_t m, const uint32_t* k, uint32_t k0,
+                                   const uint32_t* ef, uint32_t ef0,
+                                   uint32_t* ids, uint32_t kstride,
+                                   uint32_t* pool_ids, float* pool_d,
+                                   uint32_t pstride, uint32_t* stats,
+                                   void* stream);
+
+/* Waits for `stream` and reports what the device-side search recorded since
+ * the last batch started on this index: LQG_OK, or LQG_ERR_CAPACITY when a
+ * query overflowed the exact kernel's work area (its ids are LQG_NO_ID). */
+LQG_API lqg_status lqg_stream_status(lqg_index* ix, void* stream);
+
+/* The same with HOST buffers: copies in, searches, copies out, synchronizes.
+ * Pinned host memory gives the fastest copies. */
+LQG_API lqg_status lqg_search_batch(lqg_index* ix, const float* queries, int64_t m,
+                            const uint32_t* k, uint32_t k0, const uint32_t* ef,
+                            uint32_t ef0, uint32_t* ids, uint32_t kstride,
+                            uint32_t* pool_ids, float* pool_d,
+                            uint32_t pstride, uint32_t* stats, void* stream);
+
+/* Runs every query of the batch through the exact (heap-emulating) kernel
+ * only; same arguments and outputs as lqg_search_batch_device. Used to check
+ * the fast kernel and to count the reference's distance evaluations. */
+LQG_API lqg_status lqg_search_exact_device(lqg_index* ix, const float* queries,
+                                   int64_t m, const uint32_t* k, uint32_t k0,
+                                   const uint32_t* ef, uint32_t ef0,
+                                   uint32_t* ids, uint32_t kstride,
+                                   uint32_t* pool_ids, float* pool_d,
+                                   uint32_t pstride, uint32_t* stats,
+                                   void* stream);
+
+/* Launch shape of the fast kernel. 0 fields keep the autotuned default.
+ * lanes_per_cand in {1,2,4,8,16}; visited_bits in [8, 13];
+ * warps_per_block in {1..16}; blocks_per_sm in {1..32}. */
+typedef struct {
+    uint32_t lanes_per_cand;
+    uint32_t visited_bits;
+    uint32_t warps_per_block;
+    uint32_t blocks_per_sm;
+} lqg_tuning;
+
+LQG_API lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t);
+LQG_API lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t);
+
+/* Basic properties. */
+LQG_API lqg_status lqg_info(const lqg_index* ix, uint64_t* num_elements,
+                    uint32_t* dimension, uint32_t* degree_bound,
+                    uint32_t* entry, uint32_t* ef);
+
+/* Device pointers of the resident index (for callers that fuse their own
+ * work): nbrs [N][deg] u32, codes [N][cstride] u8, params [D][2] f32. */
+LQG_API lqg_status lqg_device_arrays(const lqg_index* ix, const uint32_t** nbrs,
+                             const uint8_t** codes, const float** params,
+                             uint32_t* code_stride);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

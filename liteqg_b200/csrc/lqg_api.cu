@@ -1,0 +1,685 @@
+// Host side of the B200 query path: the index object, the reference's file
+// format, and the C ABI declared in include/lqg.h.
+//
+// Device layout of a loaded index (HBM, resident for the index's lifetime):
+//   nbrs   [N][deg]      u32   neighbour ids, split out of the reference's
+//                              float rows (symqglib/qg/qg.hpp:128-137, 420-436)
+//   codes  [N][cstride]  u8    SQ8 codes, rows padded to a 16-byte multiple
+//   params [D][2]        f32   (min, scale)
+// The raw float vectors stay on the host: search never reads them
+// (qg.hpp:325-328 reads only the codes), save() writes them back.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/lqg.h"
+#include "lqg_internal.h"
+
+using lqg::ExactScratch;
+using lqg::SearchArgs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+lqg_status fail(lqg_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+lqg_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(LQG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define LQG_CUDA(call)                                      \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+// Control words in device memory, zeroed before every batch.
+enum : int { kCtlFastHead = 0, kCtlFlagged = 1, kCtlExactHead = 2, kCtlErr = 3, kCtlErrQuery = 4 };
+constexpr int kCtlWords = 8;
+
+constexpr uint32_t kMaxEf = 512;
+
+}  // namespace
+
+struct lqg_index {
+    uint64_t n = 0;
+    uint32_t dim = 0, deg = 0, cstride = 0;
+    int device = 0;
+    uint32_t entry = 0;
+    uint32_t ef = 0;  // 0 until lqg_set_ef (the reference leaves it undefined)
+    bool has_data = false;
+    int num_sms = 148;
+
+    std::vector<float> vectors;   // [n][dim]
+    std::vector<uint32_t> nbrs;   // [n][deg]
+    std::vector<uint8_t> codes;   // [n][dim]
+    std::vector<float> params;    // [dim][2]
+
+    uint32_t* d_nbrs = nullptr;
+    uint8_t* d_codes = nullptr;
+    float* d_params = nullptr;
+
+    uint32_t* d_ctl = nullptr;
+    int32_t* d_flagged = nullptr;
+    int64_t flagged_cap = 0;
+
+    ExactScratch xs{};
+    int x_warps = 0, x_blocks = 0;
+    static constexpr int kExactWarpsPerBlock = 4;
+
+    // staging for the host-buffer entry points
+    float* d_q = nullptr;
+    uint32_t* d_kq = nullptr;
+    uint32_t* d_efq = nullptr;
+    uint32_t* d_ids = nullptr;
+    uint32_t* d_pool_ids = nullptr;
+    float* d_pool_d = nullptr;
+    uint32_t* d_stats = nullptr;
+    size_t cap_q = 0, cap_kq = 0, cap_efq = 0, cap_ids = 0, cap_pool_ids = 0, cap_pool_d = 0,
+           cap_stats = 0;
+
+    cudaStream_t own_stream = nullptr;
+    lqg_tuning tune{4, 10, 8, 0};
+
+    ~lqg_index() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        dfree(d_nbrs);
+        dfree(d_codes);
+        dfree(d_params);
+        dfree(d_ctl);
+        dfree(d_flagged);
+        dfree(xs.vis);
+        dfree(xs.sp);
+        dfree(xs.rp);
+        dfree(d_q);
+        dfree(d_kq);
+        dfree(d_efq);
+        dfree(d_ids);
+        dfree(d_pool_ids);
+        dfree(d_pool_d);
+        dfree(d_stats);
+        if (own_stream) cudaStreamDestroy(own_stream);
+        cudaSetDevice(prev);
+    }
+};
+
+namespace {
+
+// Makes ix->device current for the scope of a call.
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+uint64_t file_bytes(uint64_t n, uint32_t dim, uint32_t deg) {
+    return 4 + 4ull * n * (dim + deg) + n * (uint64_t)dim + 8ull * dim;
+}
+
+lqg_status validate_content(const lqg_index* ix) {
+    if (ix->entry >= ix->n)
+        return fail(LQG_ERR_CORRUPT, "entry point " + std::to_string(ix->entry) +
+                                         " out of range (N=" + std::to_string(ix->n) + ")");
+    const uint32_t* p = ix->nbrs.data();
+    const uint64_t total = ix->n * ix->deg;
+    for (uint64_t i = 0; i < total; ++i)
+        if (p[i] >= ix->n)
+            return fail(LQG_ERR_CORRUPT, "neighbour id " + std::to_string(p[i]) + " of node " +
+                                             std::to_string(i / ix->deg) + " out of range");
+    return LQG_OK;
+}
+
+lqg_status upload(lqg_index* ix) {
+    DeviceScope ds(ix->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    dfree(ix->d_nbrs);
+    dfree(ix->d_codes);
+    dfree(ix->d_params);
+    const size_t nb = ix->n * ix->deg * sizeof(uint32_t);
+    const size_t cb = ix->n * ix->cstride;
+    if (cudaMalloc(&ix->d_nbrs, nb) != cudaSuccess || cudaMalloc(&ix->d_codes, cb) != cudaSuccess ||
+        cudaMalloc(&ix->d_params, ix->dim * 2 * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        dfree(ix->d_nbrs);
+        dfree(ix->d_codes);
+        return fail(LQG_ERR_NOMEM, "device allocation of the index failed");
+    }
+    LQG_CUDA(cudaMemcpy(ix->d_nbrs, ix->nbrs.data(), nb, cudaMemcpyHostToDevice));
+    if (ix->cstride != ix->dim) LQG_CUDA(cudaMemset(ix->d_codes, 0, cb));
+    LQG_CUDA(cudaMemcpy2D(ix->d_codes, ix->cstride, ix->codes.data(), ix->dim, ix->dim, ix->n,
+                          cudaMemcpyHostToDevice));
+    LQG_CUDA(cudaMemcpy(ix->d_params, ix->params.data(), ix->dim * 2 * sizeof(float),
+                        cudaMemcpyHostToDevice));
+    ix->has_data = true;
+    return LQG_OK;
+}
+
+int pool_regs_for(uint32_t ef_max) {
+    int e = 1;
+    while (32u * e < ef_max) e *= 2;
+    return e;
+}
+
+lqg_status ensure_ctl(lqg_index* ix, int64_t m) {
+    if (!ix->d_ctl) {
+        if (cudaMalloc(&ix->d_ctl, kCtlWords * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LQG_ERR_NOMEM, "control block allocation failed");
+        }
+    }
+    if (ix->flagged_cap < m) {
+        dfree(ix->d_flagged);
+        const int64_t cap = std::max<int64_t>(m, 1024);
+        if (cudaMalloc(&ix->d_flagged, cap * sizeof(int32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            ix->flagged_cap = 0;
+            return fail(LQG_ERR_NOMEM, "flag list allocation failed");
+        }
+        ix->flagged_cap = cap;
+    }
+    return LQG_OK;
+}
+
+// Exact-kernel work areas: a fixed set of warps, each with an exact visited
+// set of 2^16 slots (up to 32768 visited nodes per query), a search heap of
+// 32768 entries and a result heap of kMaxEf + 8 entries.
+lqg_status ensure_exact(lqg_index* ix) {
+    if (ix->xs.vis) return LQG_OK;
+    ix->x_blocks = ix->num_sms;
+    ix->x_warps = ix->x_blocks * lqg_index::kExactWarpsPerBlock;
+    ix->xs.xbits = 16;
+    ix->xs.scap = 32768;
+    ix->xs.rcap = kMaxEf + 8;
+    const size_t w = ix->x_warps;
+    if (cudaMalloc(&ix->xs.vis, w * ((size_t)1 << ix->xs.xbits) * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&ix->xs.sp, w * ix->xs.scap * sizeof(uint2)) != cudaSuccess ||
+        cudaMalloc(&ix->xs.rp, w * ix->xs.rcap * sizeof(uint2)) != cudaSuccess) {
+        cudaGetLastError();
+        dfree(ix->xs.vis);
+        dfree(ix->xs.sp);
+        dfree(ix->xs.rp);
+        return fail(LQG_ERR_NOMEM, "exact-kernel work area allocation failed");
+    }
+    return LQG_OK;
+}
+
+struct BatchSpec {
+    const float* q;
+    int64_t m;
+    const uint32_t* kq;
+    uint32_t k0;
+    const uint32_t* efq;
+    uint32_t ef0;
+    uint32_t* ids;
+    uint32_t kstride;
+    uint32_t* pool_ids;
+    float* pool_d;
+    uint32_t pstride;
+    uint32_t* stats;
+    cudaStream_t st;
+};
+
+lqg_status check_batch(lqg_index* ix, BatchSpec& b) {
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    if (!ix->has_data) return fail(LQG_ERR_STATE, "index has no data: load or build it first");
+    if (b.m < 0 || b.m > (int64_t)INT32_MAX) return fail(LQG_ERR_ARG, "bad query count");
+    if (b.m > 0 && (!b.q || !b.ids)) return fail(LQG_ERR_ARG, "null queries or ids");
+    if (!b.kq && b.k0 > b.kstride) return fail(LQG_ERR_ARG, "k exceeds kstride");
+    if (b.kstride == 0) return fail(LQG_ERR_ARG, "kstride must be > 0");
+    if (!b.efq && b.ef0 == 0) {
+        if (ix->ef == 0) return fail(LQG_ERR_STATE, "ef not set: call set_ef first");
+        b.ef0 = ix->ef;
+    }
+    if (b.ef0 == 0 || b.ef0 > kMaxEf)
+        return fail(LQG_ERR_ARG, "ef (or the per-query ef bound) must be in [1, 512]");
+    if ((b.pool_ids == nullptr) != (b.pool_d == nullptr))
+        return fail(LQG_ERR_ARG, "pool_ids and pool_d go together");
+    if (b.pool_ids && b.pstride == 0) return fail(LQG_ERR_ARG, "pstride must be > 0");
+    return LQG_OK;
+}
+
+SearchArgs base_args(const lqg_index* ix, const BatchSpec& b) {
+    SearchArgs a{};
+    a.nbrs = ix->d_nbrs;
+    a.codes = ix->d_codes;
+    a.params = ix->d_params;
+    a.n = (uint32_t)ix->n;
+    a.dim = ix->dim;
+    a.deg = ix->deg;
+    a.cstride = ix->cstride;
+    a.entry = ix->entry;
+    a.queries = b.q;
+    a.m = b.m;
+    a.kq = b.kq;
+    a.k0 = b.k0;
+    a.efq = b.efq;
+    a.ef0 = b.ef0;
+    a.ids = b.ids;
+    a.kstride = b.kstride;
+    a.pool_ids = b.pool_ids;
+    a.pool_d = b.pool_d;
+    a.pstride = b.pstride;
+    a.stats = b.stats;
+    a.err = ix->d_ctl + kCtlErr;
+    return a;
+}
+
+lqg_status reset_ctl(lqg_index* ix, cudaStream_t st) {
+    LQG_CUDA(cudaMemsetAsync(ix->d_ctl, 0, kCtlWords * sizeof(uint32_t), st));
+    LQG_CUDA(cudaMemsetAsync(ix->d_ctl + kCtlErrQuery, 0xFF, sizeof(uint32_t), st));
+    return LQG_OK;
+}
+
+// Fast kernel over all queries, then the exact kernel over the flagged ones.
+// `plain` launches one warp (the one-query-per-launch form).
+lqg_status run_batch(lqg_index* ix, BatchSpec& b, bool plain) {
+    lqg_status s = check_batch(ix, b);
+    if (s != LQG_OK) return s;
+    if (b.m == 0) return LQG_OK;
+    DeviceScope ds(ix->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    if ((s = ensure_ctl(ix, b.m)) != LQG_OK) return s;
+    if ((s = ensure_exact(ix)) != LQG_OK) return s;
+    if ((s = reset_ctl(ix, b.st)) != LQG_OK) return s;
+
+    const int E = pool_regs_for(b.ef0);
+    const int degw = (int)(ix->deg / 32);
+    const lqg_tuning& t = ix->tune;
+    SearchArgs a = base_args(ix, b);
+    a.qhead = ix->d_ctl + kCtlFastHead;
+    a.nflagged = ix->d_ctl + kCtlFlagged;
+    a.flagged = ix->d_flagged;
+    a.vbits = t.visited_bits;
+    int warps = plain ? 1 : (int)t.warps_per_block;
+    int blocks = 1;
+    if (!plain) {
+        int occ = t.blocks_per_sm ? (int)t.blocks_per_sm
+                                  : lqg::fast_occupancy(E, (int)t.lanes_per_cand, degw, warps,
+                                                        ix->dim, t.visited_bits);
+        if (occ <= 0) return fail(LQG_ERR_ARG, "fast kernel cannot launch with this tuning");
+        blocks = occ * ix->num_sms;
+        const int64_t need = (b.m + warps - 1) / warps;
+        if (need < blocks) blocks = (int)need;
+    }
+    cudaError_t e = lqg::launch_fast(a, E, (int)t.lanes_per_cand, degw, warps, blocks, b.st);
+    if (e != cudaSuccess) return cuda_fail(e, "fast search launch");
+
+    SearchArgs x = base_args(ix, b);
+    x.qlist = ix->d_flagged;
+    x.nlist = ix->d_ctl + kCtlFlagged;
+    x.qhead = ix->d_ctl + kCtlExactHead;
+    int xb = plain ? 1 : ix->x_blocks;
+    int xw = plain ? 1 : lqg_index::kExactWarpsPerBlock;
+    e = lqg::launch_exact(x, ix->xs, degw, xw, xb, b.st);
+    if (e != cudaSuccess) return cuda_fail(e, "exact search launch");
+    return LQG_OK;
+}
+
+lqg_status read_status(lqg_index* ix, cudaStream_t st) {
+    uint32_t ctl[kCtlWords];
+    LQG_CUDA(cudaMemcpyAsync(ctl, ix->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
+    LQG_CUDA(cudaStreamSynchronize(st));
+    if (ctl[kCtlErr]) {
+        std::string why;
+        if (ctl[kCtlErr] & lqg::kErrVisitedFull) why += " visited set full (32768 nodes);";
+        if (ctl[kCtlErr] & lqg::kErrHeapFull) why += " search heap full (32768 entries);";
+        if (ctl[kCtlErr] & lqg::kErrProbe) why += " visited-set probe failed;";
+        return fail(LQG_ERR_CAPACITY, "exact search work area overflow for query " +
+                                          std::to_string(ctl[kCtlErrQuery]) + ":" + why);
+    }
+    return LQG_OK;
+}
+
+template <typename T>
+lqg_status grow(T*& p, size_t& cap, size_t need) {
+    if (need <= cap) return LQG_OK;
+    dfree(p);
+    cap = 0;
+    if (cudaMalloc(&p, need * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(LQG_ERR_NOMEM, "staging allocation failed");
+    }
+    cap = need;
+    return LQG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lqg_last_error(void) { return g_last_error.c_str(); }
+
+lqg_status lqg_create(const char* index_type, const char* metric, uint64_t num_elements,
+                      uint32_t dimension, uint32_t degree_bound, int device, lqg_index** out) {
+    if (!out) return fail(LQG_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (!metric || std::string(metric) != "L2")
+        return fail(LQG_ERR_ARG, "Only L2 distance supported currently");
+    if (degree_bound < 32 || degree_bound % 32 != 0)
+        return fail(LQG_ERR_ARG, "The degree bound must be a multiple of 32");
+    if (!index_type || std::string(index_type) != "QG")
+        return fail(LQG_ERR_ARG, std::string("Index type [") + (index_type ? index_type : "") +
+                                     "] not supported");
+    if (degree_bound > lqg::kMaxDeg)
+        return fail(LQG_ERR_ARG, "degree_bound above 128 is not supported on the GPU");
+    if (dimension < 33 || dimension > 2048)
+        return fail(LQG_ERR_ARG, "dimension must be in [33, 2048]");
+    if (num_elements == 0 || num_elements >= (1ull << 31))
+        return fail(LQG_ERR_ARG, "num_elements must be in [1, 2^31)");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= ndev) return fail(LQG_ERR_ARG, "bad device ordinal");
+    auto* ix = new (std::nothrow) lqg_index();
+    if (!ix) return fail(LQG_ERR_NOMEM, "host allocation failed");
+    ix->n = num_elements;
+    ix->dim = dimension;
+    ix->deg = degree_bound;
+    ix->cstride = (dimension + 15u) & ~15u;
+    ix->device = device;
+    cudaDeviceGetAttribute(&ix->num_sms, cudaDevAttrMultiProcessorCount, device);
+    *out = ix;
+    return LQG_OK;
+}
+
+void lqg_free(lqg_index* ix) { delete ix; }
+
+lqg_status lqg_load(lqg_index* ix, const char* path) {
+    if (!ix || !path) return fail(LQG_ERR_ARG, "null argument");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(LQG_ERR_IO, std::string("cannot open ") + path);
+    std::fseek(f, 0, SEEK_END);
+    const long long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    const uint64_t want = file_bytes(ix->n, ix->dim, ix->deg);
+    if (size < 0 || (uint64_t)size != want) {
+        std::fclose(f);
+        return fail(LQG_ERR_IO, std::string(path) + ": " + std::to_string(size) +
+                                    " bytes, expected " + std::to_string(want) +
+                                    " for the index's N, dimension and degree_bound");
+    }
+    try {
+        ix->vectors.resize(ix->n * ix->dim);
+        ix->nbrs.resize(ix->n * ix->deg);
+        ix->codes.resize(ix->n * ix->dim);
+        ix->params.resize(ix->dim * 2);
+    } catch (...) {
+        std::fclose(f);
+        return fail(LQG_ERR_NOMEM, "host allocation failed");
+    }
+    bool ok = std::fread(&ix->entry, 4, 1, f) == 1;
+    const size_t row = ix->dim + ix->deg;
+    std::vector<uint32_t> buf;
+    const size_t chunk = 1 << 16;
+    for (uint64_t i0 = 0; ok && i0 < ix->n; i0 += chunk) {
+        const size_t rows = std::min<uint64_t>(chunk, ix->n - i0);
+        buf.resize(rows * row);
+        ok = std::fread(buf.data(), 4, rows * row, f) == rows * row;
+        for (size_t r = 0; ok && r < rows; ++r) {
+            std::memcpy(&ix->vectors[(i0 + r) * ix->dim], &buf[r * row], 4 * ix->dim);
+            std::memcpy(&ix->nbrs[(i0 + r) * ix->deg], &buf[r * row + ix->dim], 4 * ix->deg);
+        }
+    }
+    ok = ok && std::fread(ix->codes.data(), 1, ix->codes.size(), f) == ix->codes.size();
+    ok = ok && std::fread(ix->params.data(), 4, ix->params.size(), f) == ix->params.size();
+    std::fclose(f);
+    if (!ok) return fail(LQG_ERR_IO, std::string("short read from ") + path);
+    lqg_status s = validate_content(ix);
+    if (s != LQG_OK) return s;
+    return upload(ix);
+}
+
+lqg_status lqg_save(const lqg_index* ix, const char* path) {
+    if (!ix || !path) return fail(LQG_ERR_ARG, "null argument");
+    if (!ix->has_data) return fail(LQG_ERR_STATE, "index has no data");
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(LQG_ERR_IO, std::string("cannot create ") + path);
+    bool ok = std::fwrite(&ix->entry, 4, 1, f) == 1;
+    const size_t row = ix->dim + ix->deg;
+    std::vector<uint32_t> buf;
+    const size_t chunk = 1 << 16;
+    for (uint64_t i0 = 0; ok && i0 < ix->n; i0 += chunk) {
+        const size_t rows = std::min<uint64_t>(chunk, ix->n - i0);
+        buf.resize(rows * row);
+        for (size_t r = 0; r < rows; ++r) {
+            std::memcpy(&buf[r * row], &ix->vectors[(i0 + r) * ix->dim], 4 * ix->dim);
+            std::memcpy(&buf[r * row + ix->dim], &ix->nbrs[(i0 + r) * ix->deg], 4 * ix->deg);
+        }
+        ok = std::fwrite(buf.data(), 4, rows * row, f) == rows * row;
+    }
+    ok = ok && std::fwrite(ix->codes.data(), 1, ix->codes.size(), f) == ix->codes.size();
+    ok = ok && std::fwrite(ix->params.data(), 4, ix->params.size(), f) == ix->params.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? LQG_OK : fail(LQG_ERR_IO, std::string("write to ") + path + " failed");
+}
+
+lqg_status lqg_set_arrays(lqg_index* ix, uint32_t entry, const float* vectors,
+                          const uint32_t* nbrs, const uint8_t* codes, const float* params) {
+    if (!ix || !nbrs || !codes || !params) return fail(LQG_ERR_ARG, "null argument");
+    try {
+        ix->vectors.assign(ix->n * ix->dim, 0.f);
+        if (vectors) std::memcpy(ix->vectors.data(), vectors, ix->vectors.size() * 4);
+        ix->nbrs.assign(nbrs, nbrs + ix->n * ix->deg);
+        ix->codes.assign(codes, codes + ix->n * ix->dim);
+        ix->params.assign(params, params + ix->dim * 2);
+    } catch (...) {
+        return fail(LQG_ERR_NOMEM, "host allocation failed");
+    }
+    ix->entry = entry;
+    lqg_status s = validate_content(ix);
+    if (s != LQG_OK) return s;
+    return upload(ix);
+}
+
+lqg_status lqg_get_arrays(const lqg_index* ix, uint32_t* entry, float* vectors, uint32_t* nbrs,
+                          uint8_t* codes, float* params) {
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    if (!ix->has_data) return fail(LQG_ERR_STATE, "index has no data");
+    if (entry) *entry = ix->entry;
+    if (vectors) std::memcpy(vectors, ix->vectors.data(), ix->vectors.size() * 4);
+    if (nbrs) std::memcpy(nbrs, ix->nbrs.data(), ix->nbrs.size() * 4);
+    if (codes) std::memcpy(codes, ix->codes.data(), ix->codes.size());
+    if (params) std::memcpy(params, ix->params.data(), ix->params.size() * 4);
+    return LQG_OK;
+}
+
+lqg_status lqg_set_ef(lqg_index* ix, uint32_t ef) {
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    if (ef == 0 || ef > kMaxEf) return fail(LQG_ERR_ARG, "ef must be in [1, 512]");
+    ix->ef = ef;
+    return LQG_OK;
+}
+
+lqg_status lqg_search(lqg_index* ix, const float* query, uint32_t k, uint32_t* results) {
+    if (!ix || !query || !results) return fail(LQG_ERR_ARG, "null argument");
+    if (k == 0) return LQG_OK;
+    DeviceScope ds(ix->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    if (!ix->own_stream) LQG_CUDA(cudaStreamCreateWithFlags(&ix->own_stream, cudaStreamNonBlocking));
+    lqg_status s;
+    if ((s = grow(ix->d_q, ix->cap_q, ix->dim)) != LQG_OK) return s;
+    if ((s = grow(ix->d_ids, ix->cap_ids, k)) != LQG_OK) return s;
+    cudaStream_t st = ix->own_stream;
+    LQG_CUDA(cudaMemcpyAsync(ix->d_q, query, ix->dim * 4, cudaMemcpyHostToDevice, st));
+    BatchSpec b{ix->d_q, 1, nullptr, k, nullptr, 0, ix->d_ids, k, nullptr, nullptr, 0, nullptr, st};
+    if ((s = run_batch(ix, b, true)) != LQG_OK) return s;
+    LQG_CUDA(cudaMemcpyAsync(results, ix->d_ids, k * 4, cudaMemcpyDeviceToHost, st));
+    return read_status(ix, st);
+}
+
+lqg_status lqg_search_batch_device(lqg_index* ix, const float* queries, int64_t m,
+                                   const uint32_t* k, uint32_t k0, const uint32_t* ef,
+                                   uint32_t ef0, uint32_t* ids, uint32_t kstride,
+                                   uint32_t* pool_ids, float* pool_d, uint32_t pstride,
+                                   uint32_t* stats, void* stream) {
+    BatchSpec b{queries, m,      k,      k0,      ef,    ef0,   ids,
+                kstride, pool_ids, pool_d, pstride, stats, (cudaStream_t)stream};
+    return run_batch(ix, b, false);
+}
+
+lqg_status lqg_stream_status(lqg_index* ix, void* stream) {
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    if (!ix->d_ctl) return LQG_OK;
+    DeviceScope ds(ix->device);
+    return read_status(ix, (cudaStream_t)stream);
+}
+
+lqg_status lqg_search_batch(lqg_index* ix, const float* queries, int64_t m, const uint32_t* k,
+                            uint32_t k0, const uint32_t* ef, uint32_t ef0, uint32_t* ids,
+                            uint32_t kstride, uint32_t* pool_ids, float* pool_d,
+                            uint32_t pstride, uint32_t* stats, void* stream) {
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    if (m <= 0) return m == 0 ? LQG_OK : fail(LQG_ERR_ARG, "bad query count");
+    DeviceScope ds(ix->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t efb = ef0;
+    if (ef) {
+        efb = 0;
+        for (int64_t i = 0; i < m; ++i) efb = std::max(efb, ef[i]);
+    }
+    if (k)
+        for (int64_t i = 0; i < m; ++i)
+            if (k[i] > kstride) return fail(LQG_ERR_ARG, "k exceeds kstride");
+    lqg_status s;
+    if ((s = grow(ix->d_q, ix->cap_q, (size_t)m * ix->dim)) != LQG_OK) return s;
+    if ((s = grow(ix->d_ids, ix->cap_ids, (size_t)m * kstride)) != LQG_OK) return s;
+    if (k && (s = grow(ix->d_kq, ix->cap_kq, (size_t)m)) != LQG_OK) return s;
+    if (ef && (s = grow(ix->d_efq, ix->cap_efq, (size_t)m)) != LQG_OK) return s;
+    if (stats && (s = grow(ix->d_stats, ix->cap_stats, (size_t)m * 4)) != LQG_OK) return s;
+    if (pool_ids) {
+        if ((s = grow(ix->d_pool_ids, ix->cap_pool_ids, (size_t)m * pstride)) != LQG_OK) return s;
+        if ((s = grow(ix->d_pool_d, ix->cap_pool_d, (size_t)m * pstride)) != LQG_OK) return s;
+    }
+    LQG_CUDA(cudaMemcpyAsync(ix->d_q, queries, (size_t)m * ix->dim * 4, cudaMemcpyHostToDevice, st));
+    if (k) LQG_CUDA(cudaMemcpyAsync(ix->d_kq, k, m * 4, cudaMemcpyHostToDevice, st));
+    if (ef) LQG_CUDA(cudaMemcpyAsync(ix->d_efq, ef, m * 4, cudaMemcpyHostToDevice, st));
+    BatchSpec b{ix->d_q,
+                m,
+                k ? ix->d_kq : nullptr,
+                k0,
+                ef ? ix->d_efq : nullptr,
+                efb,
+                ix->d_ids,
+                kstride,
+                pool_ids ? ix->d_pool_ids : nullptr,
+                pool_ids ? ix->d_pool_d : nullptr,
+                pstride,
+                stats ? ix->d_stats : nullptr,
+                st};
+    if ((s = run_batch(ix, b, false)) != LQG_OK) return s;
+    LQG_CUDA(cudaMemcpyAsync(ids, ix->d_ids, (size_t)m * kstride * 4, cudaMemcpyDeviceToHost, st));
+    if (pool_ids) {
+        LQG_CUDA(cudaMemcpyAsync(pool_ids, ix->d_pool_ids, (size_t)m * pstride * 4,
+                                 cudaMemcpyDeviceToHost, st));
+        LQG_CUDA(cudaMemcpyAsync(pool_d, ix->d_pool_d, (size_t)m * pstride * 4,
+                                 cudaMemcpyDeviceToHost, st));
+    }
+    if (stats)
+        LQG_CUDA(cudaMemcpyAsync(stats, ix->d_stats, (size_t)m * 16, cudaMemcpyDeviceToHost, st));
+    return read_status(ix, st);
+}
+
+lqg_status lqg_search_exact_device(lqg_index* ix, const float* queries, int64_t m,
+                                   const uint32_t* k, uint32_t k0, const uint32_t* ef,
+                                   uint32_t ef0, uint32_t* ids, uint32_t kstride,
+                                   uint32_t* pool_ids, float* pool_d, uint32_t pstride,
+                                   uint32_t* stats, void* stream) {
+    BatchSpec b{queries, m,      k,      k0,      ef,    ef0,   ids,
+                kstride, pool_ids, pool_d, pstride, stats, (cudaStream_t)stream};
+    lqg_status s = check_batch(ix, b);
+    if (s != LQG_OK) return s;
+    if (m == 0) return LQG_OK;
+    DeviceScope ds(ix->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    if ((s = ensure_ctl(ix, 1)) != LQG_OK) return s;
+    if ((s = ensure_exact(ix)) != LQG_OK) return s;
+    if ((s = reset_ctl(ix, b.st)) != LQG_OK) return s;
+    SearchArgs x = base_args(ix, b);
+    x.qhead = ix->d_ctl + kCtlExactHead;
+    cudaError_t e = lqg::launch_exact(x, ix->xs, (int)(ix->deg / 32),
+                                      lqg_index::kExactWarpsPerBlock, ix->x_blocks, b.st);
+    if (e != cudaSuccess) return cuda_fail(e, "exact search launch");
+    return LQG_OK;
+}
+
+lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
+    if (!ix || !t) return fail(LQG_ERR_ARG, "null argument");
+    lqg_tuning n = ix->tune;
+    if (t->lanes_per_cand) {
+        const uint32_t g = t->lanes_per_cand;
+        if (g != 1 && g != 2 && g != 4 && g != 8 && g != 16)
+            return fail(LQG_ERR_ARG, "lanes_per_cand must be 1, 2, 4, 8 or 16");
+        n.lanes_per_cand = g;
+    }
+    if (t->visited_bits) {
+        if (t->visited_bits < 8 || t->visited_bits > 13)
+            return fail(LQG_ERR_ARG, "visited_bits must be in [8, 13]");
+        n.visited_bits = t->visited_bits;
+    }
+    if (t->warps_per_block) {
+        if (t->warps_per_block > 16) return fail(LQG_ERR_ARG, "warps_per_block must be <= 16");
+        n.warps_per_block = t->warps_per_block;
+    }
+    if (t->blocks_per_sm) {
+        if (t->blocks_per_sm > 32) return fail(LQG_ERR_ARG, "blocks_per_sm must be <= 32");
+        n.blocks_per_sm = t->blocks_per_sm;
+    }
+    if (lqg::fast_smem_bytes(ix->dim, n.visited_bits, (int)n.warps_per_block) > 227 * 1024)
+        return fail(LQG_ERR_ARG, "tuning needs more than 227 KB of shared memory per block");
+    ix->tune = n;
+    return LQG_OK;
+}
+
+lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t) {
+    if (!ix || !t) return fail(LQG_ERR_ARG, "null argument");
+    *t = ix->tune;
+    return LQG_OK;
+}
+
+lqg_status lqg_info(const lqg_index* ix, uint64_t* num_elements, uint32_t* dimension,
+                    uint32_t* degree_bound, uint32_t* entry, uint32_t* ef) {
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    if (num_elements) *num_elements = ix->n;
+    if (dimension) *dimension = ix->dim;
+    if (degree_bound) *degree_bound = ix->deg;
+    if (entry) *entry = ix->entry;
+    if (ef) *ef = ix->ef;
+    return LQG_OK;
+}
+
+lqg_status lqg_device_arrays(const lqg_index* ix, const uint32_t** nbrs, const uint8_t** codes,
+                             const float** params, uint32_t* code_stride) {
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    if (!ix->has_data) return fail(LQG_ERR_STATE, "index has no data");
+    if (nbrs) *nbrs = ix->d_nbrs;
+    if (codes) *codes = ix->d_codes;
+    if (params) *params = ix->d_params;
+    if (code_stride) *code_stride = ix->cstride;
+    return LQG_OK;
+}
+
+}  // extern "C"

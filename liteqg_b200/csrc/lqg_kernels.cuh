@@ -1,0 +1,185 @@
+// Device side of the B200 quantized-graph query path: shared helpers.
+//
+// Distance arithmetic restates, bit for bit, what one neighbour evaluation of
+// the reference computes (symqglib/qg/qg.hpp:325-328):
+//   dec[d]  = fma(code[d], scale[d], min[d])   (sq8.hpp:28-32, contracted by -Ofast)
+//   t       = q[d] - dec[d]
+//   acc[l]  = fma(t, t, acc[l]),  l = d % 16, in increasing d  (l2.hpp:16-35)
+//   result  = _mm512_reduce_add_ps tree: fold lanes 8..15 onto 0..7, then
+//             4..7 onto 0..3, 2..3 onto 0..1, 1 onto 0; then a scalar fma
+//             tail over d >= 16*floor(D/16).
+// A warp evaluates 32/G candidates at once: the G lanes of a group each own
+// 16/G of the 16 accumulators, and the fold tree runs across them with
+// shuffles. All arithmetic uses the _rn intrinsics, which the compiler never
+// fuses or reorders.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lqg {
+
+constexpr uint32_t kExpanded = 0x80000000u;  // pool id flag: node already popped
+constexpr uint32_t kNoId = 0xFFFFFFFFu;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr uint32_t kMaxDeg = 128;                 // degree_bound 32, 64, 96 or 128
+constexpr uint32_t kCandBytes = 8 * kMaxDeg;      // per-warp candidate staging
+
+struct SearchArgs {
+    const uint32_t* nbrs;    // [n][deg]
+    const uint8_t* codes;    // [n][cstride]
+    const float* params;     // [dim][2] (min, scale)
+    uint32_t n, dim, deg, cstride, entry;
+    const float* queries;    // [m][dim]
+    int64_t m;               // number of queries in the work list
+    const int32_t* qlist;    // work list of query indices (NULL: 0..m-1)
+    const uint32_t* nlist;   // if set, the work list length is *nlist (<= m)
+    const uint32_t* kq;      // per-query k or NULL
+    uint32_t k0;
+    const uint32_t* efq;     // per-query ef or NULL
+    uint32_t ef0;
+    uint32_t* ids;           // [.][kstride]
+    uint32_t kstride;
+    uint32_t* pool_ids;      // [.][pstride] or NULL
+    float* pool_d;
+    uint32_t pstride;
+    uint32_t* stats;         // [.][4] or NULL
+    int32_t* flagged;        // fast kernel: queries handed to the exact kernel
+    uint32_t* nflagged;
+    uint32_t* qhead;         // work-queue head (zeroed before each launch)
+    uint32_t* err;           // [0]: error bits, [1]: first failing query
+    uint32_t vbits;          // fast kernel: visited-cache bits
+};
+
+// Exact kernel work areas, one per resident warp.
+struct ExactScratch {
+    uint32_t* vis;     // [warps][1 << xbits] exact visited hash set
+    uint2* sp;         // [warps][scap]  (id, -dist bits) heap
+    uint2* rp;         // [warps][rcap]  (id, dist bits) heap
+    uint32_t xbits;
+    uint32_t scap;
+    uint32_t rcap;
+};
+
+enum : uint32_t {
+    kErrVisitedFull = 1u,
+    kErrHeapFull = 2u,
+    kErrProbe = 4u,
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ uint32_t hash_id(uint32_t v, uint32_t bits) {
+    return (v * 0x9E3779B1u) >> (32u - bits);
+}
+
+// byte t of w as an exact float: 0x4B0000bb is 2^23 + bb.
+__device__ __forceinline__ float byte_to_float(uint32_t w, int t) {
+    return __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u + t)), 8388608.0f);
+}
+
+// Loads the A = 16/G code bytes of chunk j owned by lane r of a group into w[].
+template <int A>
+__device__ __forceinline__ void load_chunk(const uint8_t* p, uint32_t (&w)[(A + 3) / 4]) {
+    if constexpr (A == 16) {
+        uint4 x = __ldg(reinterpret_cast<const uint4*>(p));
+        w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+    } else if constexpr (A == 8) {
+        uint2 x = __ldg(reinterpret_cast<const uint2*>(p));
+        w[0] = x.x; w[1] = x.y;
+    } else if constexpr (A == 4) {
+        w[0] = __ldg(reinterpret_cast<const uint32_t*>(p));
+    } else if constexpr (A == 2) {
+        w[0] = __ldg(reinterpret_cast<const unsigned short*>(p));
+    } else {
+        w[0] = __ldg(p);
+    }
+}
+
+// A consecutive floats from shared memory (16-byte aligned when A >= 4).
+template <int A>
+__device__ __forceinline__ void load_vec(const float* p, float (&v)[A]) {
+    if constexpr (A >= 4) {
+#pragma unroll
+        for (int i = 0; i < A / 4; ++i) {
+            float4 x = reinterpret_cast<const float4*>(p)[i];
+            v[4 * i] = x.x; v[4 * i + 1] = x.y; v[4 * i + 2] = x.z; v[4 * i + 3] = x.w;
+        }
+    } else if constexpr (A == 2) {
+        float2 x = *reinterpret_cast<const float2*>(p);
+        v[0] = x.x; v[1] = x.y;
+    } else {
+        v[0] = p[0];
+    }
+}
+
+// Squared L2 between the query (shared memory, qs) and the SQ8-decoded row.
+// Called by all 32 lanes together; lane r = lane % G of each group handles
+// accumulators [r*A, r*A + A). `valid` lanes load; the others compute on
+// zeros. The result is meaningful in lane r == 0 of each group.
+template <int G>
+__device__ __forceinline__ float sq8_l2_group(const uint8_t* row, bool valid,
+                                              const float* __restrict__ qs,
+                                              const float* __restrict__ pmin,
+                                              const float* __restrict__ pscale,
+                                              uint32_t dim, int r) {
+    constexpr int A = 16 / G;
+    constexpr int W = (A + 3) / 4;
+    float acc[A];
+#pragma unroll
+    for (int t = 0; t < A; ++t) acc[t] = 0.0f;
+    const uint32_t mul = dim & ~15u;
+    const uint8_t* p = row + r * A;
+    for (uint32_t base = 0; base < mul; base += 16) {
+        uint32_t w[W];
+        if (valid) {
+            load_chunk<A>(p + base, w);
+        } else {
+#pragma unroll
+            for (int i = 0; i < W; ++i) w[i] = 0;
+        }
+        const uint32_t d0 = base + r * A;
+        float qv[A], mv[A], sv[A];
+        load_vec<A>(qs + d0, qv);
+        load_vec<A>(pmin + d0, mv);
+        load_vec<A>(pscale + d0, sv);
+#pragma unroll
+        for (int t = 0; t < A; ++t) {
+            float c = byte_to_float(w[t / 4], t % 4);
+            float dec = __fmaf_rn(c, sv[t], mv[t]);
+            float df = __fsub_rn(qv[t], dec);
+            acc[t] = __fmaf_rn(df, df, acc[t]);
+        }
+    }
+    // fold tree: h = 8, 4, 2, 1
+#pragma unroll
+    for (int h = 8; h >= 1; h >>= 1) {
+        if (h >= A) {
+#pragma unroll
+            for (int t = 0; t < A; ++t) {
+                float o = __shfl_down_sync(kFull, acc[t], h / A);
+                acc[t] = __fadd_rn(acc[t], o);
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < A; ++t)
+                if (t < h) acc[t] = __fadd_rn(acc[t], acc[t + h]);
+        }
+    }
+    float res = acc[0];
+    if (mul < dim && r == 0 && valid) {
+        for (uint32_t d = mul; d < dim; ++d) {
+            float c = (float)row[d];
+            float dec = __fmaf_rn(c, pscale[d], pmin[d]);
+            float df = __fsub_rn(qs[d], dec);
+            res = __fmaf_rn(df, df, res);
+        }
+    }
+    return res;
+}
+
+}  // namespace lqg
