@@ -1,0 +1,463 @@
+// Index-build kernels: SQ8 encoding, entry point, random initial graph, and
+// the candidate pruning that turns search pools into neighbour lists.
+//
+// Reference: QGBuilder (symqglib/qg/qg_builder.hpp:48-376),
+// sq8_quantize (symqglib/quantization/sq8.hpp:11-26), compute_centroid /
+// exact_nn (symqglib/space/space.hpp:16-78).
+//
+// The SQ8 encoder reproduces the reference's file contents exactly (the codes
+// and parameters of a reference-built index are pinned by the tests): per-dim
+// min/max, scale = (max - min) * (1/255) — the reference's -Ofast build turns
+// its division by the constant 255 into that multiply — and
+// code = round_half_away((v - min) / scale) with a true division.
+//
+// Pruning follows heuristic_prune (qg_builder.hpp:155-200): candidates in
+// ascending exact distance; a candidate is kept unless an already-kept one
+// lies closer to it than the node does (d(kept, c) < d(node, c)).
+// The candidate-to-candidate distances of one node form a P x P matrix that
+// one CTA accumulates in registers over 128-dimension tiles staged in shared
+// memory.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "lqg_build.h"
+
+namespace lqg {
+
+// ---- SQ8 encode ---------------------------------------------------------
+
+__global__ void minmax_partial_kernel(const float* __restrict__ x, uint64_t n, uint32_t dim,
+                                      uint64_t rows_per_block, float* __restrict__ pmin,
+                                      float* __restrict__ pmax) {
+    const uint64_t r0 = (uint64_t)blockIdx.x * rows_per_block;
+    const uint64_t r1 = min(n, r0 + rows_per_block);
+    for (uint32_t d = threadIdx.x; d < dim; d += blockDim.x) {
+        float mn = CUDART_INF_F, mx = -CUDART_INF_F;
+        for (uint64_t i = r0; i < r1; ++i) {
+            const float v = x[i * dim + d];
+            mn = fminf(mn, v);
+            mx = fmaxf(mx, v);
+        }
+        pmin[(size_t)blockIdx.x * dim + d] = mn;
+        pmax[(size_t)blockIdx.x * dim + d] = mx;
+    }
+}
+
+__global__ void minmax_final_kernel(const float* __restrict__ pmin, const float* __restrict__ pmax,
+                                    uint32_t nblocks, uint32_t dim, float* __restrict__ params) {
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < dim; d += gridDim.x * blockDim.x) {
+        float mn = CUDART_INF_F, mx = -CUDART_INF_F;
+        for (uint32_t b = 0; b < nblocks; ++b) {
+            mn = fminf(mn, pmin[(size_t)b * dim + d]);
+            mx = fmaxf(mx, pmax[(size_t)b * dim + d]);
+        }
+        params[2 * d] = mn;
+        params[2 * d + 1] = __fmul_rn(__fsub_rn(mx, mn), 1.0f / 255.0f);
+    }
+}
+
+__global__ void sq8_encode_kernel(const float* __restrict__ x, uint64_t total, uint32_t dim,
+                                  const float* __restrict__ params, uint8_t* __restrict__ codes) {
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t d = (uint32_t)(e % dim);
+        const float mn = params[2 * d], sc = params[2 * d + 1];
+        uint8_t c = 0;
+        if (sc > 0.f) {
+            const float q = roundf(__fdiv_rn(__fsub_rn(x[e], mn), sc));
+            c = (uint8_t)fminf(fmaxf(q, 0.f), 255.f);
+        }
+        codes[e] = c;
+    }
+}
+
+// ---- entry point ----------------------------------------------------------
+
+__global__ void centroid_partial_kernel(const float* __restrict__ x, uint64_t n, uint32_t dim,
+                                        uint64_t rows_per_block, double* __restrict__ part) {
+    const uint64_t r0 = (uint64_t)blockIdx.x * rows_per_block;
+    const uint64_t r1 = min(n, r0 + rows_per_block);
+    for (uint32_t d = threadIdx.x; d < dim; d += blockDim.x) {
+        double s = 0.0;
+        for (uint64_t i = r0; i < r1; ++i) s += (double)x[i * dim + d];
+        part[(size_t)blockIdx.x * dim + d] = s;
+    }
+}
+
+__global__ void centroid_final_kernel(const double* __restrict__ part, uint32_t nblocks,
+                                      uint32_t dim, uint64_t n, float* __restrict__ centroid) {
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < dim; d += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (uint32_t b = 0; b < nblocks; ++b) s += part[(size_t)b * dim + d];
+        centroid[d] = (float)(s * (1.0 / (double)n));
+    }
+}
+
+// Squared L2 of two float vectors in the reference's 16-lane order (l2.hpp).
+__device__ __forceinline__ float l2_ref_order(const float* a, const float* b, uint32_t dim) {
+    float acc[16];
+#pragma unroll
+    for (int l = 0; l < 16; ++l) acc[l] = 0.f;
+    const uint32_t mul = dim & ~15u;
+    for (uint32_t d = 0; d < mul; d += 16) {
+#pragma unroll
+        for (int l = 0; l < 16; ++l) {
+            const float t = __fsub_rn(a[d + l], b[d + l]);
+            acc[l] = __fmaf_rn(t, t, acc[l]);
+        }
+    }
+#pragma unroll
+    for (int h = 8; h >= 1; h >>= 1)
+#pragma unroll
+        for (int l = 0; l < h; ++l) acc[l] = __fadd_rn(acc[l], acc[l + h]);
+    float r = acc[0];
+    for (uint32_t d = mul; d < dim; ++d) {
+        const float t = __fsub_rn(a[d], b[d]);
+        r = __fmaf_rn(t, t, r);
+    }
+    return r;
+}
+
+// exact_nn (space.hpp:16-48): argmin over all points of l2(x_i, centroid);
+// ties go to the smallest id. best = (distance bits << 32) | id.
+__global__ void nearest_kernel(const float* __restrict__ x, uint64_t n, uint32_t dim,
+                               const float* __restrict__ centroid,
+                               unsigned long long* __restrict__ best) {
+    unsigned long long mine = ~0ull;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float d = l2_ref_order(x + i * dim, centroid, dim);
+        const unsigned long long key = ((unsigned long long)__float_as_uint(d) << 32) | i;
+        mine = key < mine ? key : mine;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long v = __shfl_down_sync(0xFFFFFFFFu, mine, o);
+        mine = v < mine ? v : mine;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMin(best, mine);
+}
+
+// ---- random initial graph (qg_builder.hpp:263-291) -------------------------
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ uint32_t rand_id(uint64_t seed, uint64_t node, uint32_t j,
+                                            uint32_t attempt, uint64_t n) {
+    const uint64_t h = mix64(seed ^ mix64(node * 0x100000001B3ull + j * 7919u + attempt * 104729u));
+    return (uint32_t)(h % n);
+}
+
+// Fills out[node][from..deg) with distinct random ids, none equal to node or
+// to out[node][0..from). One warp per node; n > deg is required.
+__global__ void random_fill_kernel(uint32_t* __restrict__ out, const uint32_t* __restrict__ from,
+                                   uint64_t n, uint32_t deg, uint64_t seed) {
+    const uint64_t node = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (node >= n) return;
+    uint32_t* row = out + node * deg;
+    const uint32_t f = from ? min(from[node], deg) : 0u;
+    uint32_t filled = f;
+    uint32_t attempt = 0;
+    while (filled < deg) {
+        const uint32_t want = deg - filled;
+        uint32_t c = rand_id(seed, node, lane, attempt++, n);
+        bool ok = lane < (int)want && c != (uint32_t)node;
+        for (uint32_t j = 0; j < filled; ++j) ok = ok && row[j] != c;
+        const unsigned mm = __match_any_sync(0xFFFFFFFFu, ok ? c : 0xFFFFFFFFu);
+        uint32_t lt;
+        asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+        ok = ok && (mm & lt) == 0;
+        const unsigned b = __ballot_sync(0xFFFFFFFFu, ok);
+        if (ok) row[filled + __popc(b & lt)] = c;
+        filled += __popc(b);
+        __syncwarp();
+    }
+}
+
+// ---- candidate pruning ---------------------------------------------------
+
+// One CTA (kPruneThreads) per node.
+//  1. Gather candidates from up to three sources (pool rows, neighbour rows
+//     with counts, reverse rows with counts); drop the node and duplicates.
+//  2. Exact FP32 distance node -> candidate (reference 16-lane order).
+//  3. Sort ascending (bitonic, kCandMax), keep the nearest kPruneMax.
+//  4. Candidate-to-candidate distances, then the greedy RNG prune.
+//  5. Write up to deg kept ids; with fill, pad to exactly deg with the pruned
+//     candidates in distance order (the spirit of graph_refine,
+//     qg_builder.hpp:293-348) and mark the row count; rest rows receive the
+//     pruned candidates for a later fill.
+__global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t s_ids[kCandMax];
+    __shared__ float s_d[kCandMax];
+    __shared__ uint32_t s_cnt;
+    __shared__ uint8_t s_state[kPruneMax];  // 0 open, 1 kept, 2 pruned
+    float* tile = reinterpret_cast<float*>(smem);                 // [kPruneMax+1][kTileD+1]
+    float* pair = tile + (kPruneMax + 1) * (kTileD + 1);            // [kPruneMax][kPruneMax]
+
+    const uint64_t node = blockIdx.x + a.node0;
+    if (node >= a.n) return;
+    const int tid = threadIdx.x;
+    const uint32_t dim = a.dim;
+    if (tid == 0) s_cnt = 0;
+    for (int i = tid; i < kCandMax; i += kPruneThreads) {
+        s_ids[i] = 0xFFFFFFFFu;
+        s_d[i] = CUDART_INF_F;
+    }
+    __syncthreads();
+
+    // 1. gather (duplicates removed below after sorting by (id))
+    auto add = [&](uint32_t v) {
+        if (v == (uint32_t)node || v >= a.n) return;
+        const uint32_t s = atomicAdd(&s_cnt, 1u);
+        if (s < kCandMax) s_ids[s] = v;
+    };
+    if (a.pool) {
+        const uint32_t* p = a.pool + (node - a.node0) * a.pool_stride;
+        for (uint32_t j = tid; j < a.pool_take; j += kPruneThreads) add(p[j]);
+    }
+    if (a.nb) {
+        const uint32_t c = a.nb_cnt ? min(a.nb_cnt[node], a.deg) : a.deg;
+        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.nb[node * a.deg + j]);
+    }
+    if (a.rev) {
+        const uint32_t c = min(a.rev_cnt[node], a.rev_stride);
+        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.rev[node * a.rev_stride + j]);
+    }
+    __syncthreads();
+    const uint32_t cnt = min(s_cnt, (uint32_t)kCandMax);
+
+    // 2. exact distances node -> candidate (ids first sorted to drop dups)
+    // bitonic sort by id to find duplicates
+    for (uint32_t k = 2; k <= kCandMax; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = tid; i < kCandMax; i += kPruneThreads) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const uint32_t x = s_ids[i], y = s_ids[l];
+                    if ((x > y) == up) {
+                        s_ids[i] = y;
+                        s_ids[l] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const float* xn = a.x + node * dim;
+    for (uint32_t i = tid; i < cnt; i += kPruneThreads) {
+        const uint32_t v = s_ids[i];
+        const bool dup = i > 0 && s_ids[i - 1] == v;
+        s_d[i] = (dup || v == 0xFFFFFFFFu) ? CUDART_INF_F : l2_ref_order(xn, a.x + (uint64_t)v * dim, dim);
+    }
+    __syncthreads();
+    // 3. sort ascending by (distance, id)
+    for (uint32_t k = 2; k <= kCandMax; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = tid; i < kCandMax; i += kPruneThreads) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const float dx = s_d[i], dy = s_d[l];
+                    const uint32_t ix = s_ids[i], iy = s_ids[l];
+                    const bool gt = dx > dy || (dx == dy && ix > iy);
+                    if (gt == up) {
+                        s_d[i] = dy;
+                        s_d[l] = dx;
+                        s_ids[i] = iy;
+                        s_ids[l] = ix;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    uint32_t P = 0;
+    {
+        // valid candidates are the finite-distance prefix
+        __shared__ uint32_t s_valid;
+        if (tid == 0) s_valid = 0;
+        __syncthreads();
+        for (uint32_t i = tid; i < kCandMax; i += kPruneThreads)
+            if (s_d[i] < CUDART_INF_F) atomicAdd(&s_valid, 1u);
+        __syncthreads();
+        P = min(s_valid, (uint32_t)kPruneMax);
+    }
+
+    // 4. pairwise distances among the first P candidates, tiled over dims.
+    // Thread t owns pairs p = t + kPruneThreads * s of the strict upper
+    // triangle in row-major order.
+    constexpr int kPairsPerThread = (kPruneMax * (kPruneMax - 1) / 2 + kPruneThreads - 1) / kPruneThreads;
+    float acc[kPairsPerThread];
+    uint32_t pab[kPairsPerThread];  // row | col << 16
+    const uint32_t npairs = P * (P - (P > 0 ? 1 : 0)) / 2;
+#pragma unroll
+    for (int s = 0; s < kPairsPerThread; ++s) {
+        acc[s] = 0.f;
+        const uint32_t p = tid + kPruneThreads * s;
+        // invert p -> (r, c), r < c, row-major over the upper triangle of P
+        uint32_t r = 0, c = 0;
+        if (p < npairs) {
+            uint32_t rem = p;
+            uint32_t rowlen = P - 1;
+            while (rem >= rowlen) {
+                rem -= rowlen;
+                ++r;
+                --rowlen;
+            }
+            c = r + 1 + rem;
+        }
+        pab[s] = r | (c << 16);
+    }
+    for (uint32_t d0 = 0; d0 < dim; d0 += kTileD) {
+        const uint32_t td = min((uint32_t)kTileD, dim - d0);
+        __syncthreads();
+        for (uint32_t e = tid; e < P * td; e += kPruneThreads) {
+            const uint32_t r = e / td, c = e % td;
+            tile[r * (kTileD + 1) + c] = a.x[(uint64_t)s_ids[r] * dim + d0 + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < kPairsPerThread; ++s) {
+            const uint32_t p = tid + kPruneThreads * s;
+            if (p < npairs) {
+                const float* ra = tile + (pab[s] & 0xFFFFu) * (kTileD + 1);
+                const float* rb = tile + (pab[s] >> 16) * (kTileD + 1);
+                float t = acc[s];
+                for (uint32_t c = 0; c < td; ++c) {
+                    const float df = ra[c] - rb[c];
+                    t = fmaf(df, df, t);
+                }
+                acc[s] = t;
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < kPairsPerThread; ++s) {
+        const uint32_t p = tid + kPruneThreads * s;
+        if (p < npairs) pair[(pab[s] & 0xFFFFu) * kPruneMax + (pab[s] >> 16)] = acc[s];
+    }
+    for (uint32_t i = tid; i < kPruneMax; i += kPruneThreads) s_state[i] = 0;
+    __syncthreads();
+
+    // 5. greedy prune: kept j prunes later i when d(j, i) < d(node, i)
+    __shared__ uint32_t s_kept;
+    if (tid == 0) s_kept = 0;
+    __syncthreads();
+    for (uint32_t j = 0; j < P; ++j) {
+        if (s_state[j] != 0) continue;  // uniform: written before the barrier
+        if (s_kept >= a.deg) break;
+        if (tid == 0) {
+            s_state[j] = 1;
+            ++s_kept;
+        }
+        for (uint32_t i = j + 1 + tid; i < P; i += kPruneThreads)
+            if (s_state[i] == 0 && pair[j * kPruneMax + i] < s_d[i]) s_state[i] = 2;
+        __syncthreads();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t* out = a.out + node * a.deg;
+        uint32_t w = 0;
+        for (uint32_t j = 0; j < P && w < a.deg; ++j)
+            if (s_state[j] == 1) out[w++] = s_ids[j];
+        const uint32_t kept = w;
+        if (a.fill)
+            for (uint32_t j = 0; j < P && w < a.deg; ++j)
+                if (s_state[j] != 1) out[w++] = s_ids[j];
+        if (a.rest_fill) {  // caller's earlier pruned list
+            const uint32_t* rr = a.rest_fill + node * a.rest_stride;
+            const uint32_t rc = min(a.rest_fill_cnt[node], a.rest_stride);
+            for (uint32_t j = 0; j < rc && w < a.deg; ++j) {
+                const uint32_t v = rr[j];
+                bool dup = v == (uint32_t)node;
+                for (uint32_t t = 0; t < w && !dup; ++t) dup = out[t] == v;
+                if (!dup) out[w++] = v;
+            }
+        }
+        a.out_cnt[node] = w;
+        if (a.kept_cnt) a.kept_cnt[node] = kept;
+        if (a.rest) {
+            uint32_t* rr = a.rest + node * a.rest_stride;
+            uint32_t rw = 0;
+            for (uint32_t j = 0; j < P && rw < a.rest_stride; ++j)
+                if (s_state[j] != 1) rr[rw++] = s_ids[j];
+            a.rest_cnt[node] = rw;
+        }
+    }
+}
+
+size_t prune_smem_bytes() {
+    return sizeof(float) * ((size_t)(kPruneMax + 1) * (kTileD + 1) + (size_t)kPruneMax * kPruneMax);
+}
+
+// Appends node -> each of its kept neighbours' reverse lists.
+__global__ void reverse_kernel(const uint32_t* __restrict__ nb, const uint32_t* __restrict__ cnt,
+                               uint64_t n, uint32_t deg, uint32_t* __restrict__ rev,
+                               uint32_t* __restrict__ rev_cnt, uint32_t rev_stride) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t node = e / deg;
+    const uint32_t j = (uint32_t)(e % deg);
+    if (node >= n || j >= min(cnt[node], deg)) return;
+    const uint32_t v = nb[node * deg + j];
+    const uint32_t s = atomicAdd(&rev_cnt[v], 1u);
+    if (s < rev_stride) rev[(uint64_t)v * rev_stride + s] = (uint32_t)node;
+}
+
+cudaError_t launch_prune(const PruneArgs& a, uint64_t nodes, cudaStream_t st) {
+    const size_t smem = prune_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(prune_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    prune_kernel<<<(unsigned)nodes, kPruneThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sq8_encode(const float* x, uint64_t n, uint32_t dim, float* params,
+                              uint8_t* codes, float* work, cudaStream_t st) {
+    const uint32_t nb = 1024;
+    const uint64_t rpb = (n + nb - 1) / nb;
+    minmax_partial_kernel<<<nb, 128, 0, st>>>(x, n, dim, rpb, work, work + (size_t)nb * dim);
+    minmax_final_kernel<<<(dim + 127) / 128, 128, 0, st>>>(work, work + (size_t)nb * dim, nb, dim,
+                                                           params);
+    sq8_encode_kernel<<<4096, 256, 0, st>>>(x, n * dim, dim, params, codes);
+    return cudaGetLastError();
+}
+
+size_t sq8_work_floats(uint32_t dim) { return 2 * 1024 * (size_t)dim; }
+
+cudaError_t launch_entry(const float* x, uint64_t n, uint32_t dim, double* work, float* centroid,
+                         unsigned long long* best, cudaStream_t st) {
+    const uint32_t nb = 1024;
+    const uint64_t rpb = (n + nb - 1) / nb;
+    centroid_partial_kernel<<<nb, 128, 0, st>>>(x, n, dim, rpb, work);
+    centroid_final_kernel<<<(dim + 127) / 128, 128, 0, st>>>(work, nb, dim, n, centroid);
+    cudaMemsetAsync(best, 0xFF, sizeof(unsigned long long), st);
+    nearest_kernel<<<1024, 256, 0, st>>>(x, n, dim, centroid, best);
+    return cudaGetLastError();
+}
+
+size_t entry_work_doubles(uint32_t dim) { return 1024 * (size_t)dim; }
+
+cudaError_t launch_random_fill(uint32_t* out, const uint32_t* from, uint64_t n, uint32_t deg,
+                               uint64_t seed, cudaStream_t st) {
+    const uint64_t threads = n * 32;
+    random_fill_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(out, from, n, deg, seed);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reverse(const uint32_t* nb, const uint32_t* cnt, uint64_t n, uint32_t deg,
+                           uint32_t* rev, uint32_t* rev_cnt, uint32_t rev_stride, cudaStream_t st) {
+    const uint64_t total = n * deg;
+    reverse_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(nb, cnt, n, deg, rev, rev_cnt,
+                                                                    rev_stride);
+    return cudaGetLastError();
+}
+
+}  // namespace lqg
