@@ -1,0 +1,519 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 quantized-graph query path (one JSON line on stdout).
+
+Workload (default, "batched-1m128"): N = 1,000,000 base vectors, D = 128,
+float32 integers from a seeded Gaussian mixture of 1,024 isotropic clusters
+(centres uniform in [0, 255], sigma 20, clipped to [0, 255], rounded);
+degree_bound 32, build EF 400, 3 build rounds; 10,000 queries from the same
+mixture; k = 10; ef = the smallest of {64, 128, 256} whose best-10-of-pool
+recall@10 against an FP64 brute-force ground truth is >= 0.95. Synthetic data
+stands in for the reference's datasets (none ship with it).
+
+One "step" = one batched search of all 10,000 queries (one persistent launch
+of the fast kernel plus the exact kernel for tied queries), inputs resident in
+HBM. The L2 is flushed between steps (a 256 MiB write), outside the timed
+events. `e2e` times the same step through the host-buffer C-ABI call
+(lqg_search_batch): pinned host queries in, ids out, inside the timed region.
+
+The index is built on the GPU by the package's builder (the reference's own
+builder yields graphs whose recall stays far below 0.95) and cached under
+$LQG_BENCH_CACHE (default /tmp/lqg_bench) together with the ground truth, so
+the reference arm and this arm search the same index file.
+
+--impl reference: the reference's own CPU search (QuantizedGraph::search,
+compiled from its sources into oracle/_ref by oracle/Makefile; the C oracle
+port if that is absent) on all host cores, same index file, same ef and k,
+each step a bounded sample of the queries.
+
+Multi-GPU (torchrun, N > 1): replicas only. Every rank holds the same index
+and searches its own 10,000 queries (seeded by rank); no collective on the
+data path; value = all queries / max-over-ranks time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QPS @ recall@10≥0.95: batched vs plain GPU vs CPU; p50/p99 ms; HBM GB/s"
+BUILDER_VERSION = "gpu-builder-1"
+
+WORKLOADS = {
+    "batched-1m128": dict(n=1_000_000, dim=128, gen="int_mixture", clusters=1024, lo=0.0,
+                          hi=255.0, sigma=20.0, deg=32, efb=400, iters=3, nq=10_000, k=10,
+                          efs=(64, 128, 256), k_extra=100),
+    "small-100k64": dict(n=100_000, dim=64, gen="uniform", deg=32, efb=200, iters=3, nq=1000,
+                         k=10, efs=(20, 40, 60, 100, 200), k_extra=100),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------- data
+def gen_data(w, which: str, rank: int = 0):
+    """Base vectors (seed 0) or queries (seed 1, +rank for replicas)."""
+    n = w["n"] if which == "base" else w["nq"]
+    if w["gen"] == "uniform":
+        rng = np.random.default_rng(0 if which == "base" else 1 + 1000 * rank)
+        return rng.random((n, w["dim"]), dtype=np.float32)
+    centres = np.random.default_rng(0).uniform(w["lo"], w["hi"], (w["clusters"], w["dim"]))
+    rng = np.random.default_rng(100 if which == "base" else 1 + 1000 * rank)
+    out = np.empty((n, w["dim"]), dtype=np.float32)
+    step = 1 << 17
+    for s in range(0, n, step):
+        m = min(step, n - s)
+        lab = rng.integers(0, w["clusters"], m)
+        x = centres[lab] + rng.normal(0.0, w["sigma"], (m, w["dim"]))
+        out[s:s + m] = np.clip(np.rint(x), w["lo"], w["hi"])
+    return out
+
+
+def cache_dir():
+    d = os.environ.get("LQG_BENCH_CACHE", "/tmp/lqg_bench")
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def key_of(name, w):
+    h = hashlib.sha1(json.dumps([name, sorted(w.items()), BUILDER_VERSION], default=str).encode())
+    return f"{name}-{h.hexdigest()[:10]}"
+
+
+def get_index_file(name, w, base, device):
+    """Builds (GPU builder) or reuses the cached index file."""
+    import liteqg_b200
+
+    path = os.path.join(cache_dir(), key_of(name, w) + ".idx")
+    if os.path.exists(path):
+        return path, 0.0
+    ix = liteqg_b200.Index("QG", "L2", w["n"], w["dim"], w["deg"], device=device)
+    t = time.perf_counter()
+    ix.build_index(base, w["efb"], num_iter=w["iters"])
+    tb = time.perf_counter() - t
+    tmp = path + f".tmp{os.getpid()}"
+    ix.save(tmp)
+    os.replace(tmp, path)
+    ix.close()
+    return path, tb
+
+
+def ground_truth(name, w, base, queries, device, rank):
+    """FP64 brute-force top-100 ids per query (GPU, chunked), cached."""
+    import torch
+
+    path = os.path.join(cache_dir(), key_of(name, w) + f".gt{rank}.npy")
+    if os.path.exists(path):
+        return np.load(path)
+    dev = torch.device("cuda", device)
+    xb = torch.from_numpy(base).to(dev, torch.float64)
+    nb = (xb * xb).sum(1)
+    kk = 100
+    out = np.empty((len(queries), kk), np.int64)
+    for s in range(0, len(queries), 1024):
+        q = torch.from_numpy(queries[s:s + 1024]).to(dev, torch.float64)
+        d = nb[None, :] - 2.0 * (q @ xb.T) + (q * q).sum(1)[:, None]
+        out[s:s + len(q)] = torch.topk(d, kk, dim=1, largest=False).indices.cpu().numpy()
+    del xb
+    torch.cuda.empty_cache()
+    np.save(path, out)
+    return out
+
+
+def recall_at(pool_ids, gt, k):
+    hits = 0
+    for i in range(len(gt)):
+        hits += len(set(pool_ids[i, :k].tolist()) & set(gt[i, :k].tolist()))
+    return hits / (len(gt) * k)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.6)  # let the sampler start before the timed region
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per query of the fast kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "fast_search_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_reference_search(path, w, queries, k, ef, nthreads):
+    """The reference's own search (oracle/_ref) or the C oracle port."""
+    from oracle.oracle import Oracle, RefHarness, read_index, ref_available
+
+    if ref_available():
+        try:
+            h = RefHarness()
+            r = h.open(path, w["n"], w["dim"], w["deg"])
+            return (lambda q: r.search(q, k, ef, nthreads=nthreads)), "reference", r
+        except OSError:
+            pass
+    o = Oracle(read_index(path, w["n"], w["dim"], w["deg"]))
+    return (lambda q: o.search(q, k, ef, nthreads=nthreads, pool=False).compat), "port", o
+
+
+def time_cpu(fn, queries, budget_s, min_q=256):
+    """Times fn over a bounded sample sized for about budget_s seconds."""
+    s = min(min_q, len(queries))
+    t = time.perf_counter()
+    fn(queries[:s])
+    dt = time.perf_counter() - t
+    m = int(min(len(queries), max(s, s * budget_s / max(dt, 1e-6))))
+    t = time.perf_counter()
+    out = fn(queries[:m])
+    dt = time.perf_counter() - t
+    return m / dt, m, dt, out
+
+
+# ---------------------------------------------------------------- arms
+def reference_arm(args, w, name):
+    import torch
+
+    base = gen_data(w, "base")
+    queries = gen_data(w, "query")
+    path, tb = get_index_file(name, w, base, 0)
+    gt = ground_truth(name, w, base, queries, 0, 0)
+    del base
+    nthreads = os.cpu_count() or 1
+    # same ef rule as the GPU arm, decided with the reference's own pools
+    from oracle.oracle import SENTINEL
+
+    chosen, rec = w["efs"][-1], None
+    sample = queries[:2000]
+    for ef in w["efs"]:
+        fn, kind, keep = cpu_reference_search(path, w, sample, ef, ef, nthreads)
+        pool = fn(sample)  # k = ef: the whole pool, ascending
+        rec = recall_at(pool, gt[:len(sample)], w["k"])
+        if rec >= 0.95:
+            chosen = ef
+            break
+    fn, kind, keep = cpu_reference_search(path, w, queries, w["k"], chosen, nthreads)
+    per = max(256, min(len(queries), 4000))
+    for _ in range(args.warmup):
+        fn(queries[:per])
+    times = []
+    for i in range(args.steps):
+        s = (i * per) % max(1, len(queries) - per + 1)
+        t = time.perf_counter()
+        fn(queries[s:s + per])
+        times.append(time.perf_counter() - t)
+    qps = per * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{name}: reference CPU search, {per} queries per step", "ef": chosen,
+                   "k": w["k"], "recall_at_10_pool": rec, "parallelism": "host threads"},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": nthreads, "kind": kind,
+                         "sample": f"{per} of {len(queries)} queries per step, k={w['k']}, ef={chosen}"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def gpu_arm(args, w, name, rank, world, device):
+    import torch
+
+    import liteqg_b200
+    from liteqg_b200._capi import check, lib
+
+    torch.cuda.set_device(device)
+    t0 = time.perf_counter()
+    base = gen_data(w, "base")
+    queries = gen_data(w, "query", rank)
+    path, t_build = get_index_file(name, w, base, device)
+    gt = ground_truth(name, w, base, queries, device, rank)
+    log(f"[rank {rank}] data+index+gt ready in {time.perf_counter() - t0:.1f}s (build {t_build:.1f}s)")
+    n, dim, deg, nq, k = w["n"], w["dim"], w["deg"], w["nq"], w["k"]
+    ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
+    ix.load(path)
+
+    # ef selection on best-k-of-pool recall (untimed)
+    chosen, recall = None, {}
+    for ef in w["efs"]:
+        _, (pid, _) = ix.search(queries, k, ef=ef, return_pool=True)
+        recall[ef] = recall_at(pid, gt, k)
+        if recall[ef] >= 0.95 and chosen is None:
+            chosen = ef
+            break
+    if chosen is None:
+        chosen = w["efs"][-1]
+    ix.set_ef(chosen)
+
+    dev = torch.device("cuda", device)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    q_dev = torch.from_numpy(queries).to(dev)
+    ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+    # exact-kernel pass: the reference's pops/evaluations (algorithmic bytes) and
+    # a full-size parity check of the fast kernel against it
+    ids_x = torch.empty((nq, k), dtype=torch.int32, device=dev)
+    st = torch.zeros((nq, 4), dtype=torch.int32, device=dev)
+    st_fast = torch.zeros((nq, 4), dtype=torch.int32, device=dev)
+    ix.search_device(q_dev.data_ptr(), nq, k, ids_x.data_ptr(), k, ef=chosen,
+                     stats_ptr=st.data_ptr(), stream=sh, exact=True)
+    ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=chosen,
+                     stats_ptr=st_fast.data_ptr(), stream=sh)
+    ix.stream_status(sh)
+    mismatch = int((ids != ids_x).any(1).sum().item())
+    stx = st.cpu().numpy().astype(np.int64)
+    stf = st_fast.cpu().numpy().astype(np.int64)
+    pops, evals = stx[:, 0], stx[:, 1]
+    exact_share = float((stf[:, 2] == 1).mean())
+    # algorithmic bytes (per launch): neighbour rows of popped nodes, codes of
+    # evaluated nodes (+ the entry), the query; SQ8 params once per CTA
+    tune = ix.get_tuning()
+    bytes_launch = float((pops * 4 * deg + (evals + 1) * dim + 4 * dim).sum())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(evs=None):
+        if evs:
+            ix.set_kernel_events(evs[0].cuda_event, evs[1].cuda_event)
+        ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=chosen, stream=sh)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    for a, b in kev:  # materialise the handles
+        a.record(stream)
+        b.record(stream)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(device) as clk:
+        for i in range(K):
+            flush.fill_(i & 0xFF)
+            ev[i][0].record(stream)
+            step(kev[i])
+            ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+    ix.set_kernel_events(0, 0)
+    ix.stream_status(sh)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    kern_ms = [a.elapsed_time(b) for a, b in kev]
+    total_s = sum(step_ms) / 1e3
+    if world > 1:
+        t = torch.tensor([total_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_s = float(t.item())
+    value = world * nq * K / total_s
+    kern_avg_s = statistics.mean(kern_ms) / 1e3
+    achieved = bytes_launch / kern_avg_s / 1e9
+    peak, peak_kind = load_peaks()
+
+    # e2e through the host-buffer C ABI: pinned queries in, ids out
+    q_pin = torch.from_numpy(queries).pin_memory()
+    ids_pin = torch.empty((nq, k), dtype=torch.int32).pin_memory()
+    h = ix.handle
+    e2e_ms = []
+    for i in range(max(3, args.warmup) + K):
+        flush.fill_(i & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        check(lib().lqg_search_batch(h, q_pin.data_ptr(), nq, None, k, None, chosen,
+                                     ids_pin.data_ptr(), k, None, None, 0, None, sh))
+        b.record(stream)
+        b.synchronize()
+        if i >= max(3, args.warmup):
+            e2e_ms.append(a.elapsed_time(b))
+    e2e_total = sum(e2e_ms) / 1e3
+    if world > 1:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e = world * nq * K / e2e_total
+    e2e_ok = bool((ids_pin.numpy() == ids.cpu().numpy()).all())
+
+    extra = {}
+    if rank == 0 and world == 1:
+        # k = 100 at the same ef
+        ids100 = torch.empty((nq, w["k_extra"]), dtype=torch.int32, device=dev)
+        for _ in range(3):
+            ix.search_device(q_dev.data_ptr(), nq, w["k_extra"], ids100.data_ptr(), w["k_extra"],
+                             ef=max(chosen, w["k_extra"]), stream=sh)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(5):
+            ix.search_device(q_dev.data_ptr(), nq, w["k_extra"], ids100.data_ptr(), w["k_extra"],
+                             ef=max(chosen, w["k_extra"]), stream=sh)
+        b.record(stream)
+        b.synchronize()
+        extra["qps_k100"] = nq * 5 / (a.elapsed_time(b) / 1e3)
+        extra["k100_ef"] = max(chosen, w["k_extra"])
+        # plain: one query per launch through Index.search (the reference call form)
+        P = min(1000, nq)
+        lat = []
+        for i in range(P + 20):
+            t = time.perf_counter()
+            ix.search(queries[i % nq], k)
+            if i >= 20:
+                lat.append(time.perf_counter() - t)
+        plain_qps = P / sum(lat)
+        extra["plain_qps"] = plain_qps
+        extra["plain_p50_ms"] = 1e3 * float(np.percentile(lat, 50))
+        extra["plain_p99_ms"] = 1e3 * float(np.percentile(lat, 99))
+        extra["batched_over_plain"] = value / plain_qps
+        # CPU baseline: the reference's own search on the host cores, bounded sample
+        nthreads = os.cpu_count() or 1
+        fn, kind, keep = cpu_reference_search(path, w, queries, k, chosen, nthreads)
+        cpu_qps, m, dt, cpu_ids = time_cpu(fn, queries, budget_s=8.0)
+        ref_mismatch = int((cpu_ids[:m] != ids.cpu().numpy().view(np.uint32)[:m]).any(1).sum())
+        cpu = {"value": cpu_qps, "unit": "queries/s", "cores": nthreads, "kind": kind,
+               "sample": f"first {m} of {nq} queries, k={k}, ef={chosen}, {dt:.1f}s wall",
+               "ids_mismatch_vs_gpu": ref_mismatch}
+    else:
+        cpu = None
+
+    traffic = profile_traffic()
+    traffic_launch = None
+    if traffic and traffic.get("workload") == name:
+        traffic_launch = traffic["dram_bytes_per_query"] * nq
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": K,
+        "warmup": max(3, args.warmup), "ms_per_step": statistics.mean(step_ms),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']}, {nq} queries/GPU, "
+                               f"k={k}, ef={chosen}", "ef": chosen, "k": k,
+                   "recall_at_10_pool": recall.get(chosen), "recall_by_ef": recall,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                   "tuning": tune, "exact_path_share": exact_share,
+                   "fast_vs_exact_id_mismatch": mismatch, "e2e_ids_equal": e2e_ok,
+                   "pops_mean": float(pops.mean()), "evals_mean": float(evals.mean())},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic_launch, "algorithmic_bytes_per_launch": bytes_launch,
+                     "kernel_ms": statistics.mean(kern_ms),
+                     "kernel": "fast_search_kernel"},
+        "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": int(nq * dim * 4),
+                "d2h_bytes_per_step": int(nq * k * 4)},
+        "gpu_launches": 2 * K,
+        "clocks": clk.summary(),
+        "p50_ms": statistics.median(step_ms), "p99_ms": float(np.percentile(step_ms, 99)),
+        **extra,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ix.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched-1m128", choices=sorted(WORKLOADS))
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        reference_arm(args, w, args.workload)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local))
+    try:
+        gpu_arm(args, w, args.workload, rank, world, local)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

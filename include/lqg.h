@@ -81,6 +81,15 @@ LQG_API lqg_status lqg_set_arrays(lqg_index* ix, uint32_t entry, const float* ve
 LQG_API lqg_status lqg_get_arrays(const lqg_index* ix, uint32_t* entry, float* vectors,
                           uint32_t* nbrs, uint8_t* codes, float* params);
 
+/* Index.build_index(data, EF, num_iter): python/bindings.cpp:69-90 ->
+ * QGBuilder (symqglib/qg/qg_builder.hpp:48-91), built on the GPU.
+ * data: HOST [N][D] f32. EF in [1, 512], num_iter >= 2. Deterministic for a
+ * given seed (the reference seeds from std::random_device). Produces the
+ * same file layout; the graph is the GPU builder's, not bit-identical to
+ * the reference builder's. */
+LQG_API lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build,
+                             uint32_t num_iter, uint64_t seed);
+
 /* Index.set_ef: symqglib/qg/qg.hpp:226-230. ef in [1, 512]. */
 LQG_API lqg_status lqg_set_ef(lqg_index* ix, uint32_t ef);
 
@@ -152,6 +161,12 @@ typedef struct {
 
 LQG_API lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t);
 LQG_API lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t);
+
+/* Profiling hook: when both are non-NULL cudaEvent_t handles, every later
+ * batch records `start` just before and `stop` just after the fast search
+ * kernel, on the batch's stream (NULL, NULL turns it off). The events stay
+ * owned by the caller. */
+LQG_API lqg_status lqg_set_kernel_events(lqg_index* ix, void* start, void* stop);
 
 /* Basic properties. */
 LQG_API lqg_status lqg_info(const lqg_index* ix, uint64_t* num_elements,

@@ -31,6 +31,7 @@ SIGNATURES = {
     "lqg_set_arrays": (C.c_int, [_vp, C.c_uint32, _vp, _vp, _vp, _vp]),
     "lqg_get_arrays": (C.c_int, [_vp, _u32p, _vp, _vp, _vp, _vp]),
     "lqg_set_ef": (C.c_int, [_vp, C.c_uint32]),
+    "lqg_build": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64]),
     "lqg_search": (C.c_int, [_vp, _vp, C.c_uint32, _vp]),
     "lqg_search_batch_device": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
                                           _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
@@ -39,6 +40,7 @@ SIGNATURES = {
                                    _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
     "lqg_search_exact_device": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
                                           _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
+    "lqg_set_kernel_events": (C.c_int, [_vp, _vp, _vp]),
     "lqg_set_tuning": (C.c_int, [_vp, _vp]),
     "lqg_get_tuning": (C.c_int, [_vp, _vp]),
     "lqg_info": (C.c_int, [_vp, C.POINTER(C.c_uint64), _u32p, _u32p, _u32p, _u32p]),

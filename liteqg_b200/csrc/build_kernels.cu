@@ -163,7 +163,7 @@ __global__ void random_fill_kernel(uint32_t* __restrict__ out, const uint32_t* _
     const uint32_t f = from ? min(from[node], deg) : 0u;
     uint32_t filled = f;
     uint32_t attempt = 0;
-    while (filled < deg) {
+    while (filled < deg && attempt < 4096) {
         const uint32_t want = deg - filled;
         uint32_t c = rand_id(seed, node, lane, attempt++, n);
         bool ok = lane < (int)want && c != (uint32_t)node;
@@ -177,6 +177,17 @@ __global__ void random_fill_kernel(uint32_t* __restrict__ out, const uint32_t* _
         filled += __popc(b);
         __syncwarp();
     }
+    // Bounded fallback (n > deg guarantees it completes): the next ids after
+    // the node, skipping the node and ids already present.
+    if (lane == 0) {
+        for (uint64_t t = 1; filled < deg && t < n; ++t) {
+            const uint32_t c = (uint32_t)((node + t) % n);
+            bool dup = false;
+            for (uint32_t j = 0; j < filled && !dup; ++j) dup = row[j] == c;
+            if (!dup) row[filled++] = c;
+        }
+    }
+    __syncwarp();
 }
 
 // ---- candidate pruning ---------------------------------------------------

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/lqg.h"
+#include "lqg_build.h"
 #include "lqg_internal.h"
 
 using lqg::ExactScratch;
@@ -95,6 +96,7 @@ struct lqg_index {
 
     cudaStream_t own_stream = nullptr;
     lqg_tuning tune{4, 10, 8, 0};
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // recorded around the fast kernel
 
     ~lqg_index() {
         int prev = 0;
@@ -324,8 +326,10 @@ lqg_status run_batch(lqg_index* ix, BatchSpec& b, bool plain) {
         const int64_t need = (b.m + warps - 1) / warps;
         if (need < blocks) blocks = (int)need;
     }
+    if (ix->ev_start) LQG_CUDA(cudaEventRecord(ix->ev_start, b.st));
     cudaError_t e = lqg::launch_fast(a, E, (int)t.lanes_per_cand, degw, warps, blocks, b.st);
     if (e != cudaSuccess) return cuda_fail(e, "fast search launch");
+    if (ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
 
     SearchArgs x = base_args(ix, b);
     x.qlist = ix->d_flagged;
@@ -626,6 +630,14 @@ lqg_status lqg_search_exact_device(lqg_index* ix, const float* queries, int64_t 
     return LQG_OK;
 }
 
+lqg_status lqg_set_kernel_events(lqg_index* ix, void* start, void* stop) {
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    if ((start == nullptr) != (stop == nullptr)) return fail(LQG_ERR_ARG, "give both events or none");
+    ix->ev_start = (cudaEvent_t)start;
+    ix->ev_stop = (cudaEvent_t)stop;
+    return LQG_OK;
+}
+
 lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
     if (!ix || !t) return fail(LQG_ERR_ARG, "null argument");
     lqg_tuning n = ix->tune;
@@ -680,6 +692,168 @@ lqg_status lqg_device_arrays(const lqg_index* ix, const uint32_t** nbrs, const u
     if (params) *params = ix->d_params;
     if (code_stride) *code_stride = ix->cstride;
     return LQG_OK;
+}
+
+
+// Index.build_index: python/bindings.cpp:69-90 -> QGBuilder
+// (symqglib/qg/qg_builder.hpp:48-91), on the GPU:
+//   SQ8 encode, entry = exact nearest point to the FP64 centroid, random
+//   initial graph; then num_iter rounds of
+//     search   every point through the current graph (fast search kernel,
+//              pool of ef_build) — the candidate step of search_new_neighbors
+//     prune    pool + current neighbours with exact FP32 distances (RNG rule)
+//     reverse  add_reverse_edges: each kept edge offered to its target, the
+//              target's list re-pruned, then filled to exactly degree_bound
+//              with its pruned candidates and, if still short, random ids.
+lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32_t num_iter,
+                     uint64_t seed) {
+    if (!ix || !data) return fail(LQG_ERR_ARG, "null argument");
+    if (num_iter <= 1) return fail(LQG_ERR_ARG, "The number of iter for building qg should >= 3");
+    if (ef_build == 0 || ef_build > kMaxEf) return fail(LQG_ERR_ARG, "EF must be in [1, 512]");
+    if (ix->n <= ix->deg) return fail(LQG_ERR_ARG, "num_elements must exceed degree_bound");
+    DeviceScope ds(ix->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    const uint64_t n = ix->n;
+    const uint32_t dim = ix->dim, deg = ix->deg;
+    try {
+        ix->vectors.assign(data, data + n * dim);
+        ix->nbrs.resize(n * deg);
+        ix->codes.resize(n * dim);
+        ix->params.resize(dim * 2);
+    } catch (...) {
+        return fail(LQG_ERR_NOMEM, "host allocation failed");
+    }
+    ix->has_data = false;
+    dfree(ix->d_nbrs);
+    dfree(ix->d_codes);
+    dfree(ix->d_params);
+
+    const uint32_t rest_stride = 64, rev_stride = deg;
+    const uint64_t chunk = std::min<uint64_t>(n, 1u << 20);
+    float* d_x = nullptr;
+    uint8_t* d_c = nullptr;
+    void* d_work = nullptr;
+    float* d_cent = nullptr;
+    unsigned long long* d_best = nullptr;
+    uint32_t *d_kept = nullptr, *d_kept_cnt = nullptr, *d_rest = nullptr, *d_rest_cnt = nullptr;
+    uint32_t *d_rev = nullptr, *d_rev_cnt = nullptr, *d_new = nullptr, *d_new_cnt = nullptr;
+    uint32_t *d_pool = nullptr, *d_k1 = nullptr;
+    float* d_pool_d = nullptr;
+    auto cleanup = [&]() {
+        dfree(d_x); dfree(d_c); if (d_work) cudaFree(d_work); d_work = nullptr;
+        dfree(d_cent); dfree(d_best); dfree(d_kept); dfree(d_kept_cnt); dfree(d_rest);
+        dfree(d_rest_cnt); dfree(d_rev); dfree(d_rev_cnt); dfree(d_new); dfree(d_new_cnt);
+        dfree(d_pool); dfree(d_k1); dfree(d_pool_d);
+    };
+    auto alloc = [&](auto*& p, size_t bytes) {
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            return false;
+        }
+        return true;
+    };
+    const size_t work_bytes = std::max(lqg::sq8_work_floats(dim) * sizeof(float),
+                                       lqg::entry_work_doubles(dim) * sizeof(double));
+    bool ok = alloc(d_x, n * dim * 4) && alloc(ix->d_codes, n * ix->cstride) &&
+              alloc(ix->d_params, dim * 8) && alloc(ix->d_nbrs, n * deg * 4) &&
+              alloc(d_work, work_bytes) && alloc(d_cent, dim * 4) && alloc(d_best, 8) &&
+              alloc(d_kept, n * deg * 4) && alloc(d_kept_cnt, n * 4) &&
+              alloc(d_rest, n * rest_stride * 4) && alloc(d_rest_cnt, n * 4) &&
+              alloc(d_rev, n * rev_stride * 4) && alloc(d_rev_cnt, n * 4) &&
+              alloc(d_new, n * deg * 4) && alloc(d_new_cnt, n * 4) &&
+              alloc(d_pool, chunk * ef_build * 4) && alloc(d_pool_d, chunk * ef_build * 4) &&
+              alloc(d_k1, chunk * 4) && (ix->cstride == dim || alloc(d_c, n * dim));
+    if (!ok) {
+        cleanup();
+        return fail(LQG_ERR_NOMEM, "device allocation for the build failed");
+    }
+    cudaStream_t st = nullptr;
+    auto check_cuda = [&](cudaError_t e, const char* what) -> lqg_status {
+        if (e == cudaSuccess) return LQG_OK;
+        cleanup();
+        return cuda_fail(e, what);
+    };
+    lqg_status s;
+#define LQG_BCUDA(call, what) \
+    if ((s = check_cuda((call), what)) != LQG_OK) return s
+    LQG_BCUDA(cudaMemcpy(d_x, data, n * dim * 4, cudaMemcpyHostToDevice), "copy data");
+    uint8_t* codes_out = ix->cstride == dim ? ix->d_codes : d_c;
+    LQG_BCUDA(lqg::launch_sq8_encode(d_x, n, dim, ix->d_params, codes_out, (float*)d_work, st),
+              "sq8 encode");
+    if (ix->cstride != dim) {
+        LQG_BCUDA(cudaMemset(ix->d_codes, 0, n * ix->cstride), "pad codes");
+        LQG_BCUDA(cudaMemcpy2D(ix->d_codes, ix->cstride, d_c, dim, dim, n, cudaMemcpyDeviceToDevice),
+                  "pad codes");
+    }
+    LQG_BCUDA(lqg::launch_entry(d_x, n, dim, (double*)d_work, d_cent, d_best, st), "entry point");
+    unsigned long long best = 0;
+    LQG_BCUDA(cudaMemcpy(&best, d_best, 8, cudaMemcpyDeviceToHost), "entry point");
+    ix->entry = (uint32_t)(best & 0xFFFFFFFFull);
+    LQG_BCUDA(lqg::launch_random_fill(ix->d_nbrs, nullptr, n, deg, seed, st), "random graph");
+    ix->has_data = true;
+
+    for (uint32_t it = 0; it < num_iter; ++it) {
+        for (uint64_t c0 = 0; c0 < n; c0 += chunk) {
+            const uint64_t m = std::min(chunk, n - c0);
+            BatchSpec b{d_x + c0 * dim, (int64_t)m, nullptr, 1, nullptr, ef_build, d_k1, 1,
+                        d_pool, d_pool_d, ef_build, nullptr, st};
+            if ((s = run_batch(ix, b, false)) != LQG_OK) {
+                cleanup();
+                return s;
+            }
+            if ((s = read_status(ix, st)) != LQG_OK) {
+                cleanup();
+                return s;
+            }
+            lqg::PruneArgs a{};
+            a.x = d_x;
+            a.n = n;
+            a.dim = dim;
+            a.deg = deg;
+            a.node0 = c0;
+            a.pool = d_pool;
+            a.pool_stride = ef_build;
+            a.pool_take = std::min<uint32_t>(ef_build, lqg::kCandMax - deg);
+            a.nb = ix->d_nbrs;
+            a.out = d_kept;
+            a.out_cnt = d_kept_cnt;
+            a.rest = d_rest;
+            a.rest_cnt = d_rest_cnt;
+            a.rest_stride = rest_stride;
+            LQG_BCUDA(lqg::launch_prune(a, m, st), "prune");
+        }
+        LQG_BCUDA(cudaMemset(d_rev_cnt, 0, n * 4), "reverse edges");
+        LQG_BCUDA(lqg::launch_reverse(d_kept, d_kept_cnt, n, deg, d_rev, d_rev_cnt, rev_stride, st),
+                  "reverse edges");
+        lqg::PruneArgs b{};
+        b.x = d_x;
+        b.n = n;
+        b.dim = dim;
+        b.deg = deg;
+        b.node0 = 0;
+        b.nb = d_kept;
+        b.nb_cnt = d_kept_cnt;
+        b.rev = d_rev;
+        b.rev_cnt = d_rev_cnt;
+        b.rev_stride = rev_stride;
+        b.out = d_new;
+        b.out_cnt = d_new_cnt;
+        b.fill = 1;
+        b.rest_fill = d_rest;
+        b.rest_fill_cnt = d_rest_cnt;
+        b.rest_stride = rest_stride;
+        LQG_BCUDA(lqg::launch_prune(b, n, st), "merge reverse edges");
+        LQG_BCUDA(lqg::launch_random_fill(d_new, d_new_cnt, n, deg, seed + 1 + it, st), "fill");
+        LQG_BCUDA(cudaMemcpy(ix->d_nbrs, d_new, n * deg * 4, cudaMemcpyDeviceToDevice), "graph");
+    }
+    LQG_BCUDA(cudaMemcpy(ix->nbrs.data(), ix->d_nbrs, n * deg * 4, cudaMemcpyDeviceToHost), "graph");
+    LQG_BCUDA(cudaMemcpy2D(ix->codes.data(), dim, ix->d_codes, ix->cstride, dim, n,
+                           cudaMemcpyDeviceToHost), "codes");
+    LQG_BCUDA(cudaMemcpy(ix->params.data(), ix->d_params, dim * 8, cudaMemcpyDeviceToHost), "params");
+#undef LQG_BCUDA
+    cleanup();
+    return validate_content(ix);
 }
 
 }  // extern "C"

@@ -85,9 +85,9 @@ class Index:
     def set_ef(self, EF: int) -> None:
         check(lib().lqg_set_ef(self.handle, int(EF)))
 
-    def build_index(self, data, EF: int, num_iter: int = 3, num_thread: int = UINT_MAX) -> None:
-        from .builder import build_graph
-
+    def build_index(self, data, EF: int, num_iter: int = 3, num_thread: int = UINT_MAX,
+                    seed: int = 0) -> None:
+        """Builds on the GPU (``num_thread`` is accepted and unused)."""
         items = _as_f32(data)
         if items.ndim == 1:
             items = items.reshape(1, -1)
@@ -97,8 +97,7 @@ class Index:
                 f"({self.num_elements}, {self.dimension}), but got: {tuple(items.shape)}")
         if num_iter <= 1:
             raise ValueError("The number of iter for building qg should >= 3")
-        g = build_graph(items, self.degree_bound, int(EF), int(num_iter), device=self.device)
-        self.set_arrays(g.entry, items, g.nbrs, g.codes, g.params)
+        check(lib().lqg_build(self.handle, _p(items), int(EF), int(num_iter), int(seed)))
 
     def search(self, query, k: int, ef=None, return_pool: bool = False,
                return_stats: bool = False):
@@ -204,6 +203,10 @@ class Index:
         check(f(self.handle, q_ptr, m, k_ptr or None, k, ef_ptr or None, ef, ids_ptr, kstride,
                 pool_ids_ptr or None, pool_d_ptr or None, pstride, stats_ptr or None,
                 stream or None))
+
+    def set_kernel_events(self, start: int = 0, stop: int = 0) -> None:
+        """cudaEvent_t handles (ints) recorded around each fast-kernel launch."""
+        check(lib().lqg_set_kernel_events(self.handle, start or None, stop or None))
 
     def stream_status(self, stream: int = 0) -> None:
         check(lib().lqg_stream_status(self.handle, stream or None))

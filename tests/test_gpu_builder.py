@@ -1,0 +1,66 @@
+"""GPU index builder: valid graph, reference-exact SQ8 encoding, usable recall."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, read_index, sq8_quantize
+
+pytestmark = pytest.mark.gpu
+
+
+def _recall(pool, gt, k):
+    return np.mean([len(set(pool[i, :k]) & set(gt[i, :k])) / k for i in range(len(gt))])
+
+
+@pytest.mark.parametrize("n,dim,deg", [(20000, 64, 32), (8000, 96, 64), (5000, 40, 32)])
+def test_build_graph_valid_and_searchable(tmp_path, n, dim, deg):
+    import liteqg_b200
+
+    rng = np.random.default_rng(n + dim)
+    x = rng.random((n, dim), dtype=np.float32)
+    q = rng.random((200, dim), dtype=np.float32)
+    ix = liteqg_b200.Index("QG", "L2", n, dim, deg)
+    ix.build_index(x, 100, num_iter=3)
+    entry, vec, nb, codes, params = ix.get_arrays()
+    assert np.array_equal(vec, x)
+    # graph: exactly deg distinct ids per node, none the node itself
+    assert nb.shape == (n, deg) and int(nb.max()) < n
+    srt = np.sort(nb, axis=1)
+    assert not (srt[:, 1:] == srt[:, :-1]).any()
+    assert not (nb == np.arange(n, dtype=np.uint32)[:, None]).any()
+    # SQ8 encoding equals the reference encoder (pinned by the oracle tests)
+    c2, p2 = sq8_quantize(x, 2)
+    assert np.array_equal(codes, c2) and np.array_equal(params, p2)
+    # entry point: nearest point to the centroid
+    cen = (x.astype(np.float64).sum(0) / n).astype(np.float32)
+    d = ((x - cen) ** 2).sum(1)
+    assert d[entry] <= d.min() * (1 + 1e-5)
+    # searching the built index is exact against the oracle, and recall is high
+    path = str(tmp_path / "b.idx")
+    ix.save(path)
+    o = Oracle(read_index(path, n, dim, deg))
+    got, (pid, pd) = ix.search(q, 10, ef=64, return_pool=True)
+    want = o.search(q, 10, 64)
+    assert np.array_equal(got, want.compat)
+    gt = np.argsort(((q[:, None, :].astype(np.float64) - x[None].astype(np.float64)) ** 2).sum(-1), 1)[:, :10]
+    assert _recall(pid, gt, 10) > 0.9
+
+
+def test_build_is_deterministic():
+    import liteqg_b200
+
+    x = np.random.default_rng(3).random((6000, 48), dtype=np.float32)
+    a = liteqg_b200.Index("QG", "L2", 6000, 48, 32)
+    b = liteqg_b200.Index("QG", "L2", 6000, 48, 32)
+    a.build_index(x, 64, 2)
+    b.build_index(x, 64, 2)
+    assert np.array_equal(a.get_arrays()[2], b.get_arrays()[2])
+
+
+def test_build_rejects_bad_shapes():
+    import liteqg_b200
+
+    ix = liteqg_b200.Index("QG", "L2", 100, 64, 32)
+    with pytest.raises(ValueError, match="different with initialization"):
+        ix.build_index(np.zeros((99, 64), np.float32), 50)
+    with pytest.raises(ValueError, match=">= 3"):
+        ix.build_index(np.zeros((100, 64), np.float32), 50, num_iter=1)
