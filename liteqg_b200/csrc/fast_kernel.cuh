@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(512) fast_search_kernel(SearchArgs a) {
         float d0 = sq8_l2_group<G>(a.codes + (size_t)ep * a.cstride, g == 0, qs, pmin,
                                    pscale, dim, r);
         d0 = __shfl_sync(kFull, d0, 0);
-        bool tie = !(d0 < INF);
+        bool tie = !(d0 < INF) && !a.ties_ok;
         if (lane == 0) {
             pd[0] = d0;
             pi[0] = ep;
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(512) fast_search_kernel(SearchArgs a) {
                 bad |= valid && !(dc < INF);
                 key[w] = (valid && dc < T) ? __float_as_uint(dc) : 0xFFFFFFFFu;
             }
-            if (__any_sync(kFull, bad)) {
+            if (__any_sync(kFull, bad) && !a.ties_ok) {
                 tie = true;
                 break;
             }
@@ -200,28 +200,31 @@ __global__ void __launch_bounds__(512) fast_search_kernel(SearchArgs a) {
                 for (int w = 1; w < DEGW; ++w)
                     if (src_w == w) mine = cv[w];
                 const uint32_t cidv = __shfl_sync(kFull, mine, src);
+                // holders of the same id are one node: drop them; a holder
+                // with another id is a tie (left in place for ties_ok)
                 bool other = false;
 #pragma unroll
                 for (int w = 0; w < DEGW; ++w)
                     if (key[w] == mn) {
-                        other |= cv[w] != cidv;
-                        key[w] = 0xFFFFFFFFu;
+                        if (cv[w] != cidv) other = true;
+                        else key[w] = 0xFFFFFFFFu;
                     }
-                if (__any_sync(kFull, other)) {
+                if (__any_sync(kFull, other) && !a.ties_ok) {
                     tie = true;
                     break;
                 }
                 const float dmin = __uint_as_float(mn);
-                uint32_t eq = kNoId;
+                bool dup = false, teq = false;
 #pragma unroll
                 for (int t = 0; t < E; ++t)
-                    if (pd[t] == dmin) eq = pi[t] & ~kExpanded;
-                if (__any_sync(kFull, eq != kNoId)) {
-                    if (__any_sync(kFull, eq != kNoId && eq != cidv)) {
-                        tie = true;
-                        break;
+                    if (pd[t] == dmin) {
+                        if ((pi[t] & ~kExpanded) == cidv) dup = true;
+                        else teq = true;
                     }
-                    continue;  // the same node again: it is already pooled
+                if (__any_sync(kFull, dup)) continue;  // the same node again: already pooled
+                if (__any_sync(kFull, teq) && !a.ties_ok) {
+                    tie = true;
+                    break;
                 }
                 if (!(dmin < T)) break;
                 uint32_t cnt = 0;

@@ -242,6 +242,7 @@ struct BatchSpec {
     uint32_t pstride;
     uint32_t* stats;
     cudaStream_t st;
+    uint32_t ties_ok = 0;
 };
 
 lqg_status check_batch(lqg_index* ix, BatchSpec& b) {
@@ -315,6 +316,7 @@ lqg_status run_batch(lqg_index* ix, BatchSpec& b, bool plain) {
     a.nflagged = ix->d_ctl + kCtlFlagged;
     a.flagged = ix->d_flagged;
     a.vbits = t.visited_bits;
+    a.ties_ok = b.ties_ok;
     int warps = plain ? 1 : (int)t.warps_per_block;
     int blocks = 1;
     if (!plain) {
@@ -797,7 +799,7 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
         for (uint64_t c0 = 0; c0 < n; c0 += chunk) {
             const uint64_t m = std::min(chunk, n - c0);
             BatchSpec b{d_x + c0 * dim, (int64_t)m, nullptr, 1, nullptr, ef_build, d_k1, 1,
-                        d_pool, d_pool_d, ef_build, nullptr, st};
+                        d_pool, d_pool_d, ef_build, nullptr, st, 1};
             if ((s = run_batch(ix, b, false)) != LQG_OK) {
                 cleanup();
                 return s;

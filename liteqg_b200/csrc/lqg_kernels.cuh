@@ -49,6 +49,9 @@ struct SearchArgs {
     uint32_t* qhead;         // work-queue head (zeroed before each launch)
     uint32_t* err;           // [0]: error bits, [1]: first failing query
     uint32_t vbits;          // fast kernel: visited-cache bits
+    uint32_t ties_ok;        // fast kernel: resolve equal distances by insertion
+                             // order instead of handing the query to the exact
+                             // kernel (index build only; not reference order)
 };
 
 // Exact kernel work areas, one per resident warp.
