@@ -137,25 +137,37 @@ __device__ __forceinline__ float sq8_l2_group(const uint8_t* row, bool valid,
     for (int t = 0; t < A; ++t) acc[t] = 0.0f;
     const uint32_t mul = dim & ~15u;
     const uint8_t* p = row + r * A;
-    for (uint32_t base = 0; base < mul; base += 16) {
-        uint32_t w[W];
-        if (valid) {
-            load_chunk<A>(p + base, w);
-        } else {
+    // Up to U chunks of the row are requested before any arithmetic, so the
+    // global-memory latency is paid once per U chunks, not once per chunk.
+    constexpr int U = 8;
+    for (uint32_t base = 0; base < mul; base += 16 * U) {
+        uint32_t w[U][W];
 #pragma unroll
-            for (int i = 0; i < W; ++i) w[i] = 0;
+        for (int u = 0; u < U; ++u) {
+            const uint32_t b = base + 16 * u;
+            if (valid && b < mul) {
+                load_chunk<A>(p + b, w[u]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < W; ++i) w[u][i] = 0;
+            }
         }
-        const uint32_t d0 = base + r * A;
-        float qv[A], mv[A], sv[A];
-        load_vec<A>(qs + d0, qv);
-        load_vec<A>(pmin + d0, mv);
-        load_vec<A>(pscale + d0, sv);
 #pragma unroll
-        for (int t = 0; t < A; ++t) {
-            float c = byte_to_float(w[t / 4], t % 4);
-            float dec = __fmaf_rn(c, sv[t], mv[t]);
-            float df = __fsub_rn(qv[t], dec);
-            acc[t] = __fmaf_rn(df, df, acc[t]);
+        for (int u = 0; u < U; ++u) {
+            const uint32_t d0 = base + 16 * u + r * A;
+            if (base + 16 * u < mul) {
+                float qv[A], mv[A], sv[A];
+                load_vec<A>(qs + d0, qv);
+                load_vec<A>(pmin + d0, mv);
+                load_vec<A>(pscale + d0, sv);
+#pragma unroll
+                for (int t = 0; t < A; ++t) {
+                    float c = byte_to_float(w[u][t / 4], t % 4);
+                    float dec = __fmaf_rn(c, sv[t], mv[t]);
+                    float df = __fsub_rn(qv[t], dec);
+                    acc[t] = __fmaf_rn(df, df, acc[t]);
+                }
+            }
         }
     }
     // fold tree: h = 8, 4, 2, 1
