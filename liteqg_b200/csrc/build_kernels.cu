@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "lqg_build.h"
 
 namespace lqg {
@@ -237,8 +239,9 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.nb[node * a.deg + j]);
     }
     if (a.rev) {
-        const uint32_t c = min(a.rev_cnt[node], a.rev_stride);
-        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.rev[node * a.rev_stride + j]);
+        const uint32_t s0 = a.rev_start[node], s1 = a.rev_end[node];
+        const uint32_t c = min(s1 - s0, a.rev_cap);
+        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.rev[s0 + j]);
     }
     __syncthreads();
     const uint32_t cnt = min(s_cnt, (uint32_t)kCandMax);
@@ -408,17 +411,29 @@ size_t prune_smem_bytes() {
     return sizeof(float) * ((size_t)(kPruneMax + 1) * (kTileD + 1) + (size_t)kPruneMax * kPruneMax);
 }
 
-// Appends node -> each of its kept neighbours' reverse lists.
-__global__ void reverse_kernel(const uint32_t* __restrict__ nb, const uint32_t* __restrict__ cnt,
-                               uint64_t n, uint32_t deg, uint32_t* __restrict__ rev,
-                               uint32_t* __restrict__ rev_cnt, uint32_t rev_stride) {
+// Reverse lists as CSR, deterministic: pair (target, source) for every kept
+// edge at a fixed position, a stable radix sort by target, then each target's
+// segment [start, end) of sources in ascending source order.
+__global__ void reverse_pairs_kernel(const uint32_t* __restrict__ nb,
+                                     const uint32_t* __restrict__ cnt, uint64_t n, uint32_t deg,
+                                     uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * deg) return;
     const uint64_t node = e / deg;
     const uint32_t j = (uint32_t)(e % deg);
-    if (node >= n || j >= min(cnt[node], deg)) return;
-    const uint32_t v = nb[node * deg + j];
-    const uint32_t s = atomicAdd(&rev_cnt[v], 1u);
-    if (s < rev_stride) rev[(uint64_t)v * rev_stride + s] = (uint32_t)node;
+    const bool ok = j < min(cnt[node], deg);
+    keys[e] = ok ? nb[e] : 0xFFFFFFFFu;
+    vals[e] = (uint32_t)node;
+}
+
+__global__ void segment_kernel(const uint32_t* __restrict__ keys, uint64_t total, uint64_t n,
+                               uint32_t* __restrict__ start, uint32_t* __restrict__ end) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const uint32_t k = keys[i];
+    if (k >= n) return;
+    if (i == 0 || keys[i - 1] != k) start[k] = (uint32_t)i;
+    if (i + 1 == total || keys[i + 1] != k) end[k] = (uint32_t)(i + 1);
 }
 
 cudaError_t launch_prune(const PruneArgs& a, uint64_t nodes, cudaStream_t st) {
@@ -463,11 +478,25 @@ cudaError_t launch_random_fill(uint32_t* out, const uint32_t* from, uint64_t n, 
     return cudaGetLastError();
 }
 
+size_t reverse_temp_bytes(uint64_t n, uint32_t deg) {
+    size_t t = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)(n * deg));
+    return t;
+}
+
 cudaError_t launch_reverse(const uint32_t* nb, const uint32_t* cnt, uint64_t n, uint32_t deg,
-                           uint32_t* rev, uint32_t* rev_cnt, uint32_t rev_stride, cudaStream_t st) {
+                           ReverseWork& w, cudaStream_t st) {
     const uint64_t total = n * deg;
-    reverse_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(nb, cnt, n, deg, rev, rev_cnt,
-                                                                    rev_stride);
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    reverse_pairs_kernel<<<blocks, 256, 0, st>>>(nb, cnt, n, deg, w.keys_in, w.vals_in);
+    size_t tb = w.temp_bytes;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(w.temp, tb, w.keys_in, w.keys_out, w.vals_in,
+                                                    w.vals_out, (int)total, 0, 32, st);
+    if (e != cudaSuccess) return e;
+    cudaMemsetAsync(w.start, 0, n * sizeof(uint32_t), st);
+    cudaMemsetAsync(w.end, 0, n * sizeof(uint32_t), st);
+    segment_kernel<<<blocks, 256, 0, st>>>(w.keys_out, total, n, w.start, w.end);
     return cudaGetLastError();
 }
 

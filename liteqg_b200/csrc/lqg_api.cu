@@ -730,7 +730,7 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
     dfree(ix->d_codes);
     dfree(ix->d_params);
 
-    const uint32_t rest_stride = 64, rev_stride = deg;
+    const uint32_t rest_stride = 64, rev_cap = deg;
     const uint64_t chunk = std::min<uint64_t>(n, 1u << 20);
     float* d_x = nullptr;
     uint8_t* d_c = nullptr;
@@ -738,13 +738,16 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
     float* d_cent = nullptr;
     unsigned long long* d_best = nullptr;
     uint32_t *d_kept = nullptr, *d_kept_cnt = nullptr, *d_rest = nullptr, *d_rest_cnt = nullptr;
-    uint32_t *d_rev = nullptr, *d_rev_cnt = nullptr, *d_new = nullptr, *d_new_cnt = nullptr;
+    uint32_t *d_new = nullptr, *d_new_cnt = nullptr;
+    lqg::ReverseWork rw{};
     uint32_t *d_pool = nullptr, *d_k1 = nullptr;
     float* d_pool_d = nullptr;
     auto cleanup = [&]() {
         dfree(d_x); dfree(d_c); if (d_work) cudaFree(d_work); d_work = nullptr;
         dfree(d_cent); dfree(d_best); dfree(d_kept); dfree(d_kept_cnt); dfree(d_rest);
-        dfree(d_rest_cnt); dfree(d_rev); dfree(d_rev_cnt); dfree(d_new); dfree(d_new_cnt);
+        dfree(d_rest_cnt); dfree(d_new); dfree(d_new_cnt);
+        dfree(rw.keys_in); dfree(rw.vals_in); dfree(rw.keys_out); dfree(rw.vals_out);
+        dfree(rw.start); dfree(rw.end); if (rw.temp) cudaFree(rw.temp); rw.temp = nullptr;
         dfree(d_pool); dfree(d_k1); dfree(d_pool_d);
     };
     auto alloc = [&](auto*& p, size_t bytes) {
@@ -762,7 +765,10 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
               alloc(d_work, work_bytes) && alloc(d_cent, dim * 4) && alloc(d_best, 8) &&
               alloc(d_kept, n * deg * 4) && alloc(d_kept_cnt, n * 4) &&
               alloc(d_rest, n * rest_stride * 4) && alloc(d_rest_cnt, n * 4) &&
-              alloc(d_rev, n * rev_stride * 4) && alloc(d_rev_cnt, n * 4) &&
+              alloc(rw.keys_in, n * deg * 4) && alloc(rw.vals_in, n * deg * 4) &&
+              alloc(rw.keys_out, n * deg * 4) && alloc(rw.vals_out, n * deg * 4) &&
+              alloc(rw.start, n * 4) && alloc(rw.end, n * 4) &&
+              alloc(rw.temp, (rw.temp_bytes = lqg::reverse_temp_bytes(n, deg)) + 256) &&
               alloc(d_new, n * deg * 4) && alloc(d_new_cnt, n * 4) &&
               alloc(d_pool, chunk * ef_build * 4) && alloc(d_pool_d, chunk * ef_build * 4) &&
               alloc(d_k1, chunk * 4) && (ix->cstride == dim || alloc(d_c, n * dim));
@@ -825,9 +831,7 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
             a.rest_stride = rest_stride;
             LQG_BCUDA(lqg::launch_prune(a, m, st), "prune");
         }
-        LQG_BCUDA(cudaMemset(d_rev_cnt, 0, n * 4), "reverse edges");
-        LQG_BCUDA(lqg::launch_reverse(d_kept, d_kept_cnt, n, deg, d_rev, d_rev_cnt, rev_stride, st),
-                  "reverse edges");
+        LQG_BCUDA(lqg::launch_reverse(d_kept, d_kept_cnt, n, deg, rw, st), "reverse edges");
         lqg::PruneArgs b{};
         b.x = d_x;
         b.n = n;
@@ -836,9 +840,10 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
         b.node0 = 0;
         b.nb = d_kept;
         b.nb_cnt = d_kept_cnt;
-        b.rev = d_rev;
-        b.rev_cnt = d_rev_cnt;
-        b.rev_stride = rev_stride;
+        b.rev = rw.vals_out;
+        b.rev_start = rw.start;
+        b.rev_end = rw.end;
+        b.rev_cap = rev_cap;
         b.out = d_new;
         b.out_cnt = d_new_cnt;
         b.fill = 1;

@@ -21,9 +21,10 @@ struct PruneArgs {
     uint32_t pool_stride, pool_take;
     const uint32_t* nb;      // [n][deg]
     const uint32_t* nb_cnt;  // [n] or null (= deg)
-    const uint32_t* rev;     // [n][rev_stride]
-    const uint32_t* rev_cnt;
-    uint32_t rev_stride;
+    const uint32_t* rev;        // reverse sources, CSR values
+    const uint32_t* rev_start;  // [n] segment start in rev
+    const uint32_t* rev_end;    // [n] segment end
+    uint32_t rev_cap;           // sources taken per node (lowest ids first)
     // outputs
     uint32_t* out;       // [n][deg]
     uint32_t* out_cnt;   // [n] ids written
@@ -45,7 +46,14 @@ size_t entry_work_doubles(uint32_t dim);
 cudaError_t launch_random_fill(uint32_t* out, const uint32_t* from, uint64_t n, uint32_t deg,
                                uint64_t seed, cudaStream_t st);
 cudaError_t launch_prune(const PruneArgs& a, uint64_t nodes, cudaStream_t st);
+struct ReverseWork {
+    uint32_t *keys_in, *vals_in, *keys_out, *vals_out;  // [n * deg] each
+    uint32_t *start, *end;                              // [n] each
+    void* temp;
+    size_t temp_bytes;
+};
+size_t reverse_temp_bytes(uint64_t n, uint32_t deg);
 cudaError_t launch_reverse(const uint32_t* nb, const uint32_t* cnt, uint64_t n, uint32_t deg,
-                           uint32_t* rev, uint32_t* rev_cnt, uint32_t rev_stride, cudaStream_t st);
+                           ReverseWork& w, cudaStream_t st);
 
 }  // namespace lqg
