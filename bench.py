@@ -306,6 +306,7 @@ def gpu_arm(args, w, name, rank, world, device):
     n, dim, deg, nq, k = w["n"], w["dim"], w["deg"], w["nq"], w["k"]
     ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
     ix.load(path)
+    log(f"[rank {rank}] index loaded {time.perf_counter() - t0:.1f}s")
 
     # ef selection on best-k-of-pool recall (untimed)
     chosen, recall = None, {}
@@ -318,6 +319,7 @@ def gpu_arm(args, w, name, rank, world, device):
     if chosen is None:
         chosen = w["efs"][-1]
     ix.set_ef(chosen)
+    log(f"[rank {rank}] ef={chosen} recall={recall} {time.perf_counter() - t0:.1f}s")
 
     dev = torch.device("cuda", device)
     stream = torch.cuda.current_stream(dev)
@@ -371,6 +373,7 @@ def gpu_arm(args, w, name, rank, world, device):
         torch.cuda.synchronize(dev)
     ix.set_kernel_events(0, 0)
     ix.stream_status(sh)
+    log(f"[rank {rank}] timed loop done {time.perf_counter() - t0:.1f}s")
     step_ms = [a.elapsed_time(b) for a, b in ev]
     kern_ms = [a.elapsed_time(b) for a, b in kev]
     total_s = sum(step_ms) / 1e3
@@ -406,6 +409,7 @@ def gpu_arm(args, w, name, rank, world, device):
     e2e = world * nq * K / e2e_total
     e2e_ok = bool((ids_pin.numpy() == ids.cpu().numpy()).all())
 
+    log(f"[rank {rank}] e2e done {time.perf_counter() - t0:.1f}s")
     extra = {}
     if rank == 0 and world == 1:
         # k = 100 at the same ef
@@ -435,6 +439,7 @@ def gpu_arm(args, w, name, rank, world, device):
         extra["plain_p50_ms"] = 1e3 * float(np.percentile(lat, 50))
         extra["plain_p99_ms"] = 1e3 * float(np.percentile(lat, 99))
         extra["batched_over_plain"] = value / plain_qps
+        log(f"[rank {rank}] plain done {time.perf_counter() - t0:.1f}s")
         # CPU baseline: the reference's own search on the host cores, bounded sample
         nthreads = os.cpu_count() or 1
         fn, kind, keep = cpu_reference_search(path, w, queries, k, chosen, nthreads)

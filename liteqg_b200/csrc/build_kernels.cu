@@ -209,7 +209,8 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     __shared__ uint32_t s_ids[kCandMax];
     __shared__ float s_d[kCandMax];
     __shared__ uint32_t s_cnt;
-    __shared__ uint8_t s_state[kPruneMax];  // 0 open, 1 kept, 2 pruned
+    __shared__ uint8_t s_state[kPruneMax];  // 0 open, 2 pruned
+    __shared__ uint8_t s_keep[kPruneMax];   // 1 kept
     float* tile = reinterpret_cast<float*>(smem);                 // [kPruneMax+1][kTileD+1]
     float* pair = tile + (kPruneMax + 1) * (kTileD + 1);            // [kPruneMax][kPruneMax]
 
@@ -357,20 +358,24 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         const uint32_t p = tid + kPruneThreads * s;
         if (p < npairs) pair[(pab[s] & 0xFFFFu) * kPruneMax + (pab[s] >> 16)] = acc[s];
     }
-    for (uint32_t i = tid; i < kPruneMax; i += kPruneThreads) s_state[i] = 0;
+    for (uint32_t i = tid; i < kPruneMax; i += kPruneThreads) {
+        s_state[i] = 0;
+        s_keep[i] = 0;
+    }
     __syncthreads();
 
-    // 5. greedy prune: kept j prunes later i when d(j, i) < d(node, i)
-    __shared__ uint32_t s_kept;
-    if (tid == 0) s_kept = 0;
-    __syncthreads();
+    // 5. greedy prune: kept j prunes later i when d(j, i) < d(node, i).
+    // s_state[i] only ever goes 0 -> 2 (pruned), written for i > j by the
+    // thread that owns i and read at the top of later iterations, after the
+    // barrier; kept marks go to s_keep, which the loop never reads; every
+    // thread counts kept candidates in a register, so all threads take the
+    // same branches.
+    uint32_t kept_n = 0;
     for (uint32_t j = 0; j < P; ++j) {
-        if (s_state[j] != 0) continue;  // uniform: written before the barrier
-        if (s_kept >= a.deg) break;
-        if (tid == 0) {
-            s_state[j] = 1;
-            ++s_kept;
-        }
+        if (s_state[j] != 0) continue;
+        if (kept_n >= a.deg) break;
+        ++kept_n;
+        if (tid == 0) s_keep[j] = 1;
         for (uint32_t i = j + 1 + tid; i < P; i += kPruneThreads)
             if (s_state[i] == 0 && pair[j * kPruneMax + i] < s_d[i]) s_state[i] = 2;
         __syncthreads();
@@ -380,11 +385,11 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         uint32_t* out = a.out + node * a.deg;
         uint32_t w = 0;
         for (uint32_t j = 0; j < P && w < a.deg; ++j)
-            if (s_state[j] == 1) out[w++] = s_ids[j];
+            if (s_keep[j]) out[w++] = s_ids[j];
         const uint32_t kept = w;
         if (a.fill)
             for (uint32_t j = 0; j < P && w < a.deg; ++j)
-                if (s_state[j] != 1) out[w++] = s_ids[j];
+                if (!s_keep[j]) out[w++] = s_ids[j];
         if (a.rest_fill) {  // caller's earlier pruned list
             const uint32_t* rr = a.rest_fill + node * a.rest_stride;
             const uint32_t rc = min(a.rest_fill_cnt[node], a.rest_stride);
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
             uint32_t* rr = a.rest + node * a.rest_stride;
             uint32_t rw = 0;
             for (uint32_t j = 0; j < P && rw < a.rest_stride; ++j)
-                if (s_state[j] != 1) rr[rw++] = s_ids[j];
+                if (!s_keep[j]) rr[rw++] = s_ids[j];
             a.rest_cnt[node] = rw;
         }
     }
