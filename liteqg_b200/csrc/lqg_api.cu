@@ -19,14 +19,14 @@
 
 #include "../../include/lqg.h"
 #include "lqg_build.h"
+#include "lqg_host.h"
 #include "lqg_internal.h"
 
-using lqg::ExactScratch;
-using lqg::SearchArgs;
+namespace lqg_host {
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
 lqg_status fail(lqg_status s, const std::string& msg) {
     g_last_error = msg;
@@ -37,105 +37,7 @@ lqg_status cuda_fail(cudaError_t e, const char* what) {
     return fail(LQG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define LQG_CUDA(call)                                      \
-    do {                                                    \
-        cudaError_t e_ = (call);                            \
-        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
-    } while (0)
-
-template <typename T>
-void dfree(T*& p) {
-    if (p) cudaFree(p);
-    p = nullptr;
-}
-
-// Control words in device memory, zeroed before every batch.
-enum : int { kCtlFastHead = 0, kCtlFlagged = 1, kCtlExactHead = 2, kCtlErr = 3, kCtlErrQuery = 4 };
-constexpr int kCtlWords = 8;
-
-constexpr uint32_t kMaxEf = 512;
-
-}  // namespace
-
-struct lqg_index {
-    uint64_t n = 0;
-    uint32_t dim = 0, deg = 0, cstride = 0;
-    int device = 0;
-    uint32_t entry = 0;
-    uint32_t ef = 0;  // 0 until lqg_set_ef (the reference leaves it undefined)
-    bool has_data = false;
-    int num_sms = 148;
-
-    std::vector<float> vectors;   // [n][dim]
-    std::vector<uint32_t> nbrs;   // [n][deg]
-    std::vector<uint8_t> codes;   // [n][dim]
-    std::vector<float> params;    // [dim][2]
-
-    uint32_t* d_nbrs = nullptr;
-    uint8_t* d_codes = nullptr;
-    float* d_params = nullptr;
-
-    uint32_t* d_ctl = nullptr;
-    int32_t* d_flagged = nullptr;
-    int64_t flagged_cap = 0;
-
-    ExactScratch xs{};
-    int x_warps = 0, x_blocks = 0;
-    static constexpr int kExactWarpsPerBlock = 4;
-
-    // staging for the host-buffer entry points
-    float* d_q = nullptr;
-    uint32_t* d_kq = nullptr;
-    uint32_t* d_efq = nullptr;
-    uint32_t* d_ids = nullptr;
-    uint32_t* d_pool_ids = nullptr;
-    float* d_pool_d = nullptr;
-    uint32_t* d_stats = nullptr;
-    size_t cap_q = 0, cap_kq = 0, cap_efq = 0, cap_ids = 0, cap_pool_ids = 0, cap_pool_d = 0,
-           cap_stats = 0;
-
-    cudaStream_t own_stream = nullptr;
-    lqg_tuning tune{4, 10, 8, 0};
-    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // recorded around the fast kernel
-
-    ~lqg_index() {
-        int prev = 0;
-        cudaGetDevice(&prev);
-        cudaSetDevice(device);
-        dfree(d_nbrs);
-        dfree(d_codes);
-        dfree(d_params);
-        dfree(d_ctl);
-        dfree(d_flagged);
-        dfree(xs.vis);
-        dfree(xs.sp);
-        dfree(xs.rp);
-        dfree(d_q);
-        dfree(d_kq);
-        dfree(d_efq);
-        dfree(d_ids);
-        dfree(d_pool_ids);
-        dfree(d_pool_d);
-        dfree(d_stats);
-        if (own_stream) cudaStreamDestroy(own_stream);
-        cudaSetDevice(prev);
-    }
-};
-
-namespace {
-
-// Makes ix->device current for the scope of a call.
-struct DeviceScope {
-    int prev = -1;
-    cudaError_t err = cudaSuccess;
-    explicit DeviceScope(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) err = cudaSetDevice(dev);
-    }
-    ~DeviceScope() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
+const char* last_error() { return g_last_error.c_str(); }
 
 uint64_t file_bytes(uint64_t n, uint32_t dim, uint32_t deg) {
     return 4 + 4ull * n * (dim + deg) + n * (uint64_t)dim + 8ull * dim;
@@ -185,65 +87,49 @@ int pool_regs_for(uint32_t ef_max) {
     return e;
 }
 
-lqg_status ensure_ctl(lqg_index* ix, int64_t m) {
-    if (!ix->d_ctl) {
-        if (cudaMalloc(&ix->d_ctl, kCtlWords * sizeof(uint32_t)) != cudaSuccess) {
+lqg_status ensure_ctl(Workspace& w, int64_t m) {
+    if (!w.d_ctl) {
+        if (cudaMalloc(&w.d_ctl, kCtlWords * sizeof(uint32_t)) != cudaSuccess) {
             cudaGetLastError();
             return fail(LQG_ERR_NOMEM, "control block allocation failed");
         }
     }
-    if (ix->flagged_cap < m) {
-        dfree(ix->d_flagged);
+    if (w.flagged_cap < m) {
+        dfree(w.d_flagged);
         const int64_t cap = std::max<int64_t>(m, 1024);
-        if (cudaMalloc(&ix->d_flagged, cap * sizeof(int32_t)) != cudaSuccess) {
+        if (cudaMalloc(&w.d_flagged, cap * sizeof(int32_t)) != cudaSuccess) {
             cudaGetLastError();
-            ix->flagged_cap = 0;
+            w.flagged_cap = 0;
             return fail(LQG_ERR_NOMEM, "flag list allocation failed");
         }
-        ix->flagged_cap = cap;
+        w.flagged_cap = cap;
     }
     return LQG_OK;
 }
 
-// Exact-kernel work areas: a fixed set of warps, each with an exact visited
-// set of 2^16 slots (up to 32768 visited nodes per query), a search heap of
-// 32768 entries and a result heap of kMaxEf + 8 entries.
-lqg_status ensure_exact(lqg_index* ix) {
-    if (ix->xs.vis) return LQG_OK;
-    ix->x_blocks = ix->num_sms;
-    ix->x_warps = ix->x_blocks * lqg_index::kExactWarpsPerBlock;
-    ix->xs.xbits = 16;
-    ix->xs.scap = 32768;
-    ix->xs.rcap = kMaxEf + 8;
-    const size_t w = ix->x_warps;
-    if (cudaMalloc(&ix->xs.vis, w * ((size_t)1 << ix->xs.xbits) * sizeof(uint32_t)) != cudaSuccess ||
-        cudaMalloc(&ix->xs.sp, w * ix->xs.scap * sizeof(uint2)) != cudaSuccess ||
-        cudaMalloc(&ix->xs.rp, w * ix->xs.rcap * sizeof(uint2)) != cudaSuccess) {
+// Exact-kernel work areas: blocks x warps_per_block warps, each with an exact
+// visited set of 2^16 slots (up to 32768 visited nodes per query), a search
+// heap of 32768 entries and a result heap of kMaxEf + 8 entries (about
+// 0.5 MB per warp).
+lqg_status ensure_exact(Workspace& w, int blocks, int warps_per_block) {
+    if (w.xs.vis) return LQG_OK;
+    w.x_blocks = blocks;
+    w.x_warps_per_block = warps_per_block;
+    w.xs.xbits = 16;
+    w.xs.scap = 32768;
+    w.xs.rcap = kMaxEf + 8;
+    const size_t nw = (size_t)blocks * warps_per_block;
+    if (cudaMalloc(&w.xs.vis, nw * ((size_t)1 << w.xs.xbits) * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&w.xs.sp, nw * w.xs.scap * sizeof(uint2)) != cudaSuccess ||
+        cudaMalloc(&w.xs.rp, nw * w.xs.rcap * sizeof(uint2)) != cudaSuccess) {
         cudaGetLastError();
-        dfree(ix->xs.vis);
-        dfree(ix->xs.sp);
-        dfree(ix->xs.rp);
+        dfree(w.xs.vis);
+        dfree(w.xs.sp);
+        dfree(w.xs.rp);
         return fail(LQG_ERR_NOMEM, "exact-kernel work area allocation failed");
     }
     return LQG_OK;
 }
-
-struct BatchSpec {
-    const float* q;
-    int64_t m;
-    const uint32_t* kq;
-    uint32_t k0;
-    const uint32_t* efq;
-    uint32_t ef0;
-    uint32_t* ids;
-    uint32_t kstride;
-    uint32_t* pool_ids;
-    float* pool_d;
-    uint32_t pstride;
-    uint32_t* stats;
-    cudaStream_t st;
-    uint32_t ties_ok = 0;
-};
 
 lqg_status check_batch(lqg_index* ix, BatchSpec& b) {
     if (!ix) return fail(LQG_ERR_ARG, "null index");
@@ -264,7 +150,7 @@ lqg_status check_batch(lqg_index* ix, BatchSpec& b) {
     return LQG_OK;
 }
 
-SearchArgs base_args(const lqg_index* ix, const BatchSpec& b) {
+SearchArgs base_args(const lqg_index* ix, const Workspace& w, const BatchSpec& b) {
     SearchArgs a{};
     a.nbrs = ix->d_nbrs;
     a.codes = ix->d_codes;
@@ -286,35 +172,35 @@ SearchArgs base_args(const lqg_index* ix, const BatchSpec& b) {
     a.pool_d = b.pool_d;
     a.pstride = b.pstride;
     a.stats = b.stats;
-    a.err = ix->d_ctl + kCtlErr;
+    a.err = w.d_ctl + kCtlErr;
     return a;
 }
 
-lqg_status reset_ctl(lqg_index* ix, cudaStream_t st) {
-    LQG_CUDA(cudaMemsetAsync(ix->d_ctl, 0, kCtlWords * sizeof(uint32_t), st));
-    LQG_CUDA(cudaMemsetAsync(ix->d_ctl + kCtlErrQuery, 0xFF, sizeof(uint32_t), st));
+lqg_status reset_ctl(Workspace& w, cudaStream_t st) {
+    LQG_CUDA(cudaMemsetAsync(w.d_ctl, 0, kCtlWords * sizeof(uint32_t), st));
+    LQG_CUDA(cudaMemsetAsync(w.d_ctl + kCtlErrQuery, 0xFF, sizeof(uint32_t), st));
     return LQG_OK;
 }
 
 // Fast kernel over all queries, then the exact kernel over the flagged ones.
 // `plain` launches one warp (the one-query-per-launch form).
-lqg_status run_batch(lqg_index* ix, BatchSpec& b, bool plain) {
+lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     lqg_status s = check_batch(ix, b);
     if (s != LQG_OK) return s;
     if (b.m == 0) return LQG_OK;
     DeviceScope ds(ix->device);
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
-    if ((s = ensure_ctl(ix, b.m)) != LQG_OK) return s;
-    if ((s = ensure_exact(ix)) != LQG_OK) return s;
-    if ((s = reset_ctl(ix, b.st)) != LQG_OK) return s;
+    if ((s = ensure_ctl(w, b.m)) != LQG_OK) return s;
+    if ((s = ensure_exact(w, ix->num_sms, 4)) != LQG_OK) return s;
+    if ((s = reset_ctl(w, b.st)) != LQG_OK) return s;
 
     const int E = pool_regs_for(b.ef0);
     const int degw = (int)(ix->deg / 32);
     const lqg_tuning& t = ix->tune;
-    SearchArgs a = base_args(ix, b);
-    a.qhead = ix->d_ctl + kCtlFastHead;
-    a.nflagged = ix->d_ctl + kCtlFlagged;
-    a.flagged = ix->d_flagged;
+    SearchArgs a = base_args(ix, w, b);
+    a.qhead = w.d_ctl + kCtlFastHead;
+    a.nflagged = w.d_ctl + kCtlFlagged;
+    a.flagged = w.d_flagged;
     a.vbits = t.visited_bits;
     a.ties_ok = b.ties_ok;
     int warps = plain ? 1 : (int)t.warps_per_block;
@@ -333,20 +219,20 @@ lqg_status run_batch(lqg_index* ix, BatchSpec& b, bool plain) {
     if (e != cudaSuccess) return cuda_fail(e, "fast search launch");
     if (ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
 
-    SearchArgs x = base_args(ix, b);
-    x.qlist = ix->d_flagged;
-    x.nlist = ix->d_ctl + kCtlFlagged;
-    x.qhead = ix->d_ctl + kCtlExactHead;
-    int xb = plain ? 1 : ix->x_blocks;
-    int xw = plain ? 1 : lqg_index::kExactWarpsPerBlock;
-    e = lqg::launch_exact(x, ix->xs, degw, xw, xb, b.st);
+    SearchArgs x = base_args(ix, w, b);
+    x.qlist = w.d_flagged;
+    x.nlist = w.d_ctl + kCtlFlagged;
+    x.qhead = w.d_ctl + kCtlExactHead;
+    int xb = plain ? 1 : w.x_blocks;
+    int xw = plain ? 1 : w.x_warps_per_block;
+    e = lqg::launch_exact(x, w.xs, degw, xw, xb, b.st);
     if (e != cudaSuccess) return cuda_fail(e, "exact search launch");
     return LQG_OK;
 }
 
-lqg_status read_status(lqg_index* ix, cudaStream_t st) {
+lqg_status read_status(Workspace& w, cudaStream_t st) {
     uint32_t ctl[kCtlWords];
-    LQG_CUDA(cudaMemcpyAsync(ctl, ix->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
+    LQG_CUDA(cudaMemcpyAsync(ctl, w.d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
     LQG_CUDA(cudaStreamSynchronize(st));
     if (ctl[kCtlErr]) {
         std::string why;
@@ -359,24 +245,57 @@ lqg_status read_status(lqg_index* ix, cudaStream_t st) {
     return LQG_OK;
 }
 
-template <typename T>
-lqg_status grow(T*& p, size_t& cap, size_t need) {
-    if (need <= cap) return LQG_OK;
-    dfree(p);
-    cap = 0;
-    if (cudaMalloc(&p, need * sizeof(T)) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(LQG_ERR_NOMEM, "staging allocation failed");
+// Host-buffer batch: copy in, search, copy out, wait (one workspace).
+lqg_status search_host(lqg_index* ix, Workspace& w, const float* queries, int64_t m,
+                       const uint32_t* k, uint32_t k0, const uint32_t* ef, uint32_t efb,
+                       uint32_t* ids, uint32_t kstride, uint32_t* pool_ids, float* pool_d,
+                       uint32_t pstride, uint32_t* stats, cudaStream_t st) {
+    lqg_status s;
+    if ((s = grow(w.d_q, w.cap_q, (size_t)m * ix->dim)) != LQG_OK) return s;
+    if ((s = grow(w.d_ids, w.cap_ids, (size_t)m * kstride)) != LQG_OK) return s;
+    if (k && (s = grow(w.d_kq, w.cap_kq, (size_t)m)) != LQG_OK) return s;
+    if (ef && (s = grow(w.d_efq, w.cap_efq, (size_t)m)) != LQG_OK) return s;
+    if (stats && (s = grow(w.d_stats, w.cap_stats, (size_t)m * 4)) != LQG_OK) return s;
+    if (pool_ids) {
+        if ((s = grow(w.d_pool_ids, w.cap_pool_ids, (size_t)m * pstride)) != LQG_OK) return s;
+        if ((s = grow(w.d_pool_d, w.cap_pool_d, (size_t)m * pstride)) != LQG_OK) return s;
     }
-    cap = need;
-    return LQG_OK;
+    LQG_CUDA(cudaMemcpyAsync(w.d_q, queries, (size_t)m * ix->dim * 4, cudaMemcpyHostToDevice, st));
+    if (k) LQG_CUDA(cudaMemcpyAsync(w.d_kq, k, m * 4, cudaMemcpyHostToDevice, st));
+    if (ef) LQG_CUDA(cudaMemcpyAsync(w.d_efq, ef, m * 4, cudaMemcpyHostToDevice, st));
+    BatchSpec b{w.d_q,
+                m,
+                k ? w.d_kq : nullptr,
+                k0,
+                ef ? w.d_efq : nullptr,
+                efb,
+                w.d_ids,
+                kstride,
+                pool_ids ? w.d_pool_ids : nullptr,
+                pool_ids ? w.d_pool_d : nullptr,
+                pstride,
+                stats ? w.d_stats : nullptr,
+                st};
+    if ((s = run_batch(ix, w, b, false)) != LQG_OK) return s;
+    LQG_CUDA(cudaMemcpyAsync(ids, w.d_ids, (size_t)m * kstride * 4, cudaMemcpyDeviceToHost, st));
+    if (pool_ids) {
+        LQG_CUDA(cudaMemcpyAsync(pool_ids, w.d_pool_ids, (size_t)m * pstride * 4,
+                                 cudaMemcpyDeviceToHost, st));
+        LQG_CUDA(cudaMemcpyAsync(pool_d, w.d_pool_d, (size_t)m * pstride * 4,
+                                 cudaMemcpyDeviceToHost, st));
+    }
+    if (stats)
+        LQG_CUDA(cudaMemcpyAsync(stats, w.d_stats, (size_t)m * 16, cudaMemcpyDeviceToHost, st));
+    return read_status(w, st);
 }
 
-}  // namespace
+}  // namespace lqg_host
+
+using namespace lqg_host;
 
 extern "C" {
 
-const char* lqg_last_error(void) { return g_last_error.c_str(); }
+const char* lqg_last_error(void) { return lqg_host::last_error(); }
 
 lqg_status lqg_create(const char* index_type, const char* metric, uint64_t num_elements,
                       uint32_t dimension, uint32_t degree_bound, int device, lqg_index** out) {
@@ -526,14 +445,15 @@ lqg_status lqg_search(lqg_index* ix, const float* query, uint32_t k, uint32_t* r
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
     if (!ix->own_stream) LQG_CUDA(cudaStreamCreateWithFlags(&ix->own_stream, cudaStreamNonBlocking));
     lqg_status s;
-    if ((s = grow(ix->d_q, ix->cap_q, ix->dim)) != LQG_OK) return s;
-    if ((s = grow(ix->d_ids, ix->cap_ids, k)) != LQG_OK) return s;
+    Workspace& w = ix->ws;
+    if ((s = grow(w.d_q, w.cap_q, ix->dim)) != LQG_OK) return s;
+    if ((s = grow(w.d_ids, w.cap_ids, k)) != LQG_OK) return s;
     cudaStream_t st = ix->own_stream;
-    LQG_CUDA(cudaMemcpyAsync(ix->d_q, query, ix->dim * 4, cudaMemcpyHostToDevice, st));
-    BatchSpec b{ix->d_q, 1, nullptr, k, nullptr, 0, ix->d_ids, k, nullptr, nullptr, 0, nullptr, st};
-    if ((s = run_batch(ix, b, true)) != LQG_OK) return s;
-    LQG_CUDA(cudaMemcpyAsync(results, ix->d_ids, k * 4, cudaMemcpyDeviceToHost, st));
-    return read_status(ix, st);
+    LQG_CUDA(cudaMemcpyAsync(w.d_q, query, ix->dim * 4, cudaMemcpyHostToDevice, st));
+    BatchSpec b{w.d_q, 1, nullptr, k, nullptr, 0, w.d_ids, k, nullptr, nullptr, 0, nullptr, st};
+    if ((s = run_batch(ix, w, b, true)) != LQG_OK) return s;
+    LQG_CUDA(cudaMemcpyAsync(results, w.d_ids, k * 4, cudaMemcpyDeviceToHost, st));
+    return read_status(w, st);
 }
 
 lqg_status lqg_search_batch_device(lqg_index* ix, const float* queries, int64_t m,
@@ -543,14 +463,15 @@ lqg_status lqg_search_batch_device(lqg_index* ix, const float* queries, int64_t 
                                    uint32_t* stats, void* stream) {
     BatchSpec b{queries, m,      k,      k0,      ef,    ef0,   ids,
                 kstride, pool_ids, pool_d, pstride, stats, (cudaStream_t)stream};
-    return run_batch(ix, b, false);
+    if (!ix) return fail(LQG_ERR_ARG, "null index");
+    return run_batch(ix, ix->ws, b, false);
 }
 
 lqg_status lqg_stream_status(lqg_index* ix, void* stream) {
     if (!ix) return fail(LQG_ERR_ARG, "null index");
-    if (!ix->d_ctl) return LQG_OK;
+    if (!ix->ws.d_ctl) return LQG_OK;
     DeviceScope ds(ix->device);
-    return read_status(ix, (cudaStream_t)stream);
+    return read_status(ix->ws, (cudaStream_t)stream);
 }
 
 lqg_status lqg_search_batch(lqg_index* ix, const float* queries, int64_t m, const uint32_t* k,
@@ -570,43 +491,8 @@ lqg_status lqg_search_batch(lqg_index* ix, const float* queries, int64_t m, cons
     if (k)
         for (int64_t i = 0; i < m; ++i)
             if (k[i] > kstride) return fail(LQG_ERR_ARG, "k exceeds kstride");
-    lqg_status s;
-    if ((s = grow(ix->d_q, ix->cap_q, (size_t)m * ix->dim)) != LQG_OK) return s;
-    if ((s = grow(ix->d_ids, ix->cap_ids, (size_t)m * kstride)) != LQG_OK) return s;
-    if (k && (s = grow(ix->d_kq, ix->cap_kq, (size_t)m)) != LQG_OK) return s;
-    if (ef && (s = grow(ix->d_efq, ix->cap_efq, (size_t)m)) != LQG_OK) return s;
-    if (stats && (s = grow(ix->d_stats, ix->cap_stats, (size_t)m * 4)) != LQG_OK) return s;
-    if (pool_ids) {
-        if ((s = grow(ix->d_pool_ids, ix->cap_pool_ids, (size_t)m * pstride)) != LQG_OK) return s;
-        if ((s = grow(ix->d_pool_d, ix->cap_pool_d, (size_t)m * pstride)) != LQG_OK) return s;
-    }
-    LQG_CUDA(cudaMemcpyAsync(ix->d_q, queries, (size_t)m * ix->dim * 4, cudaMemcpyHostToDevice, st));
-    if (k) LQG_CUDA(cudaMemcpyAsync(ix->d_kq, k, m * 4, cudaMemcpyHostToDevice, st));
-    if (ef) LQG_CUDA(cudaMemcpyAsync(ix->d_efq, ef, m * 4, cudaMemcpyHostToDevice, st));
-    BatchSpec b{ix->d_q,
-                m,
-                k ? ix->d_kq : nullptr,
-                k0,
-                ef ? ix->d_efq : nullptr,
-                efb,
-                ix->d_ids,
-                kstride,
-                pool_ids ? ix->d_pool_ids : nullptr,
-                pool_ids ? ix->d_pool_d : nullptr,
-                pstride,
-                stats ? ix->d_stats : nullptr,
-                st};
-    if ((s = run_batch(ix, b, false)) != LQG_OK) return s;
-    LQG_CUDA(cudaMemcpyAsync(ids, ix->d_ids, (size_t)m * kstride * 4, cudaMemcpyDeviceToHost, st));
-    if (pool_ids) {
-        LQG_CUDA(cudaMemcpyAsync(pool_ids, ix->d_pool_ids, (size_t)m * pstride * 4,
-                                 cudaMemcpyDeviceToHost, st));
-        LQG_CUDA(cudaMemcpyAsync(pool_d, ix->d_pool_d, (size_t)m * pstride * 4,
-                                 cudaMemcpyDeviceToHost, st));
-    }
-    if (stats)
-        LQG_CUDA(cudaMemcpyAsync(stats, ix->d_stats, (size_t)m * 16, cudaMemcpyDeviceToHost, st));
-    return read_status(ix, st);
+    return search_host(ix, ix->ws, queries, m, k, k0, ef, efb, ids, kstride, pool_ids, pool_d,
+                       pstride, stats, st);
 }
 
 lqg_status lqg_search_exact_device(lqg_index* ix, const float* queries, int64_t m,
@@ -621,13 +507,14 @@ lqg_status lqg_search_exact_device(lqg_index* ix, const float* queries, int64_t 
     if (m == 0) return LQG_OK;
     DeviceScope ds(ix->device);
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
-    if ((s = ensure_ctl(ix, 1)) != LQG_OK) return s;
-    if ((s = ensure_exact(ix)) != LQG_OK) return s;
-    if ((s = reset_ctl(ix, b.st)) != LQG_OK) return s;
-    SearchArgs x = base_args(ix, b);
-    x.qhead = ix->d_ctl + kCtlExactHead;
-    cudaError_t e = lqg::launch_exact(x, ix->xs, (int)(ix->deg / 32),
-                                      lqg_index::kExactWarpsPerBlock, ix->x_blocks, b.st);
+    Workspace& w = ix->ws;
+    if ((s = ensure_ctl(w, 1)) != LQG_OK) return s;
+    if ((s = ensure_exact(w, ix->num_sms, 4)) != LQG_OK) return s;
+    if ((s = reset_ctl(w, b.st)) != LQG_OK) return s;
+    SearchArgs x = base_args(ix, w, b);
+    x.qhead = w.d_ctl + kCtlExactHead;
+    cudaError_t e = lqg::launch_exact(x, w.xs, (int)(ix->deg / 32), w.x_warps_per_block,
+                                      w.x_blocks, b.st);
     if (e != cudaSuccess) return cuda_fail(e, "exact search launch");
     return LQG_OK;
 }
@@ -806,11 +693,11 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
             const uint64_t m = std::min(chunk, n - c0);
             BatchSpec b{d_x + c0 * dim, (int64_t)m, nullptr, 1, nullptr, ef_build, d_k1, 1,
                         d_pool, d_pool_d, ef_build, nullptr, st, 1};
-            if ((s = run_batch(ix, b, false)) != LQG_OK) {
+            if ((s = run_batch(ix, ix->ws, b, false)) != LQG_OK) {
                 cleanup();
                 return s;
             }
-            if ((s = read_status(ix, st)) != LQG_OK) {
+            if ((s = read_status(ix->ws, st)) != LQG_OK) {
                 cleanup();
                 return s;
             }

@@ -1,0 +1,171 @@
+// Host-side internals shared by the C-ABI implementation (lqg_api.cu) and the
+// serving loop (lqg_server.cu): the index object, per-batch workspaces, and
+// the batch launcher.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/lqg.h"
+#include "lqg_internal.h"
+
+namespace lqg_host {
+
+using lqg::ExactScratch;
+using lqg::SearchArgs;
+
+lqg_status fail(lqg_status s, const std::string& msg);
+lqg_status cuda_fail(cudaError_t e, const char* what);
+
+#define LQG_CUDA(call)                                                \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return ::lqg_host::cuda_fail(e_, #call); \
+    } while (0)
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+// Control words in device memory, zeroed before every batch.
+enum : int { kCtlFastHead = 0, kCtlFlagged = 1, kCtlExactHead = 2, kCtlErr = 3, kCtlErrQuery = 4 };
+constexpr int kCtlWords = 8;
+
+constexpr uint32_t kMaxEf = 512;
+
+// Mutable device state of one batch in flight: control words, the list of
+// tie-flagged queries, the exact kernel's work areas, and staging buffers for
+// the host-buffer entry points. Batches that overlap (on different streams)
+// each need their own.
+struct Workspace {
+    uint32_t* d_ctl = nullptr;
+    int32_t* d_flagged = nullptr;
+    int64_t flagged_cap = 0;
+    ExactScratch xs{};
+    int x_blocks = 0, x_warps_per_block = 4;
+    float* d_q = nullptr;
+    uint32_t* d_kq = nullptr;
+    uint32_t* d_efq = nullptr;
+    uint32_t* d_ids = nullptr;
+    uint32_t* d_pool_ids = nullptr;
+    float* d_pool_d = nullptr;
+    uint32_t* d_stats = nullptr;
+    size_t cap_q = 0, cap_kq = 0, cap_efq = 0, cap_ids = 0, cap_pool_ids = 0, cap_pool_d = 0,
+           cap_stats = 0;
+    void release() {
+        dfree(d_ctl);
+        dfree(d_flagged);
+        flagged_cap = 0;
+        dfree(xs.vis);
+        dfree(xs.sp);
+        dfree(xs.rp);
+        dfree(d_q);
+        dfree(d_kq);
+        dfree(d_efq);
+        dfree(d_ids);
+        dfree(d_pool_ids);
+        dfree(d_pool_d);
+        dfree(d_stats);
+        cap_q = cap_kq = cap_efq = cap_ids = cap_pool_ids = cap_pool_d = cap_stats = 0;
+    }
+};
+
+// Makes ix->device current for the scope of a call.
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+struct BatchSpec {
+    const float* q;
+    int64_t m;
+    const uint32_t* kq;
+    uint32_t k0;
+    const uint32_t* efq;
+    uint32_t ef0;
+    uint32_t* ids;
+    uint32_t kstride;
+    uint32_t* pool_ids;
+    float* pool_d;
+    uint32_t pstride;
+    uint32_t* stats;
+    cudaStream_t st;
+    uint32_t ties_ok = 0;
+};
+
+template <typename T>
+lqg_status grow(T*& p, size_t& cap, size_t need) {
+    if (need <= cap) return LQG_OK;
+    dfree(p);
+    cap = 0;
+    if (cudaMalloc(&p, need * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(LQG_ERR_NOMEM, "staging allocation failed");
+    }
+    cap = need;
+    return LQG_OK;
+}
+
+lqg_status ensure_ctl(Workspace& w, int64_t m);
+lqg_status ensure_exact(Workspace& w, int blocks, int warps_per_block);
+lqg_status reset_ctl(Workspace& w, cudaStream_t st);
+lqg_status read_status(Workspace& w, cudaStream_t st);
+
+}  // namespace lqg_host
+
+struct lqg_index {
+    uint64_t n = 0;
+    uint32_t dim = 0, deg = 0, cstride = 0;
+    int device = 0;
+    uint32_t entry = 0;
+    uint32_t ef = 0;  // 0 until lqg_set_ef (the reference leaves it undefined)
+    bool has_data = false;
+    int num_sms = 148;
+
+    std::vector<float> vectors;   // [n][dim]
+    std::vector<uint32_t> nbrs;   // [n][deg]
+    std::vector<uint8_t> codes;   // [n][dim]
+    std::vector<float> params;    // [dim][2]
+
+    uint32_t* d_nbrs = nullptr;
+    uint8_t* d_codes = nullptr;
+    float* d_params = nullptr;
+
+    lqg_host::Workspace ws;  // the default work area (one batch at a time)
+
+    cudaStream_t own_stream = nullptr;
+    lqg_tuning tune{4, 10, 8, 0};
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // recorded around the fast kernel
+
+    ~lqg_index() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        lqg_host::dfree(d_nbrs);
+        lqg_host::dfree(d_codes);
+        lqg_host::dfree(d_params);
+        ws.release();
+        if (own_stream) cudaStreamDestroy(own_stream);
+        cudaSetDevice(prev);
+    }
+};
+
+namespace lqg_host {
+lqg_status check_batch(lqg_index* ix, BatchSpec& b);
+lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain);
+lqg_status search_host(lqg_index* ix, Workspace& w, const float* queries, int64_t m,
+                       const uint32_t* k, uint32_t k0, const uint32_t* ef, uint32_t efb,
+                       uint32_t* ids, uint32_t kstride, uint32_t* pool_ids, float* pool_d,
+                       uint32_t pstride, uint32_t* stats, cudaStream_t st);
+}  // namespace lqg_host
