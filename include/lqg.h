@@ -149,6 +149,27 @@ LQG_API lqg_status lqg_search_exact_device(lqg_index* ix, const float* queries,
                                    uint32_t pstride, uint32_t* stats,
                                    void* stream);
 
+/* The exact kernel with NO allocation: this entry point has no counterpart in
+ * the reference. It is for callers that cannot let a library allocate GPU
+ * memory — applications whose device memory is already reserved by another
+ * allocator (a framework's caching pool), and latency-sensitive loops where a
+ * cudaMalloc/cudaFree could synchronize the device and stall other streams.
+ * Same arguments and outputs as lqg_search_exact_device (DEVICE pointers), but
+ * the work areas live in a fixed array inside the library (about 1.1 MB per
+ * GPU, held until the process exits): ef <= 512, at most 8192 visited nodes
+ * and 8192 search-heap entries per query (else LQG_ERR_CAPACITY and that
+ * query's ids are LQG_NO_ID). The call waits for `stream` before returning.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture. All calls share the array, so calls
+ * that overlap on the GPU (other threads or streams) race: serialize them. */
+LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
+                                           int64_t m, const uint32_t* k, uint32_t k0,
+                                           const uint32_t* ef, uint32_t ef0,
+                                           uint32_t* ids, uint32_t kstride,
+                                           uint32_t* pool_ids, float* pool_d,
+                                           uint32_t pstride, uint32_t* stats,
+                                           void* stream);
+
 /* Launch shape of the fast kernel. 0 fields keep the autotuned default.
  * lanes_per_cand in {1,2,4,8,16}; visited_bits in [8, 13];
  * warps_per_block in {1..16}; blocks_per_sm in {1..32}. */

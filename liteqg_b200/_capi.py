@@ -40,6 +40,8 @@ SIGNATURES = {
                                    _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
     "lqg_search_exact_device": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
                                           _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
+    "lqg_search_exact_noalloc": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
+                                           _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
     "lqg_set_kernel_events": (C.c_int, [_vp, _vp, _vp]),
     "lqg_set_tuning": (C.c_int, [_vp, _vp]),
     "lqg_get_tuning": (C.c_int, [_vp, _vp]),
