@@ -84,11 +84,14 @@ LQG_API lqg_status lqg_get_arrays(const lqg_index* ix, uint32_t* entry, float* v
 /* Index.build_index(data, EF, num_iter): python/bindings.cpp:69-90 ->
  * QGBuilder (symqglib/qg/qg_builder.hpp:48-91), built on the GPU.
  * data: HOST [N][D] f32. EF in [1, 512], num_iter >= 2. Deterministic for a
- * given seed (the reference seeds from std::random_device). Produces the
- * same file layout; the graph is the GPU builder's, not bit-identical to
- * the reference builder's. */
+ * given seed (the reference seeds from std::random_device). random_edges
+ * (< degree_bound) slots of every list are seeded random long-range links
+ * (the reference's builder keeps leftover random links in slots its pruning
+ * leaves empty, qg.hpp:475-487); they keep well-separated clusters reachable
+ * from the single entry point. Produces the same file layout; the graph is
+ * the GPU builder's, not bit-identical to the reference builder's. */
 LQG_API lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build,
-                             uint32_t num_iter, uint64_t seed);
+                             uint32_t num_iter, uint64_t seed, uint32_t random_edges);
 
 /* Index.set_ef: symqglib/qg/qg.hpp:226-230. ef in [1, 512]. */
 LQG_API lqg_status lqg_set_ef(lqg_index* ix, uint32_t ef);
@@ -113,7 +116,9 @@ LQG_API lqg_status lqg_search(lqg_index* ix, const float* query, uint32_t k,
  *   pool_ids [m][pstride] u32, pool_d [m][pstride] f32: the full final pool
  *            in ascending distance (NULL to skip); unused slots LQG_NO_ID/inf
  *   stats    [m][4] u32 (NULL to skip): pops, distance computations,
- *            exact-path flag, pool size
+ *            kernel that finished the query (0 fast, 1 heap, 2 global exact;
+ *            the global exact kernel counts exactly the reference's
+ *            evaluations, the others also count re-evaluations), pool size
  * Queries whose pool meets two equal distances are re-run by the exact
  * kernel (libstdc++ heap order) inside the same call, so ids always equal the
  * reference's. */
@@ -170,14 +175,25 @@ LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
                                            uint32_t pstride, uint32_t* stats,
                                            void* stream);
 
-/* Launch shape of the fast kernel. 0 fields keep the autotuned default.
- * lanes_per_cand in {1,2,4,8,16}; visited_bits in [8, 13];
- * warps_per_block in {1..16}; blocks_per_sm in {1..32}. */
+/* Launch shape and policy. 0 fields keep the current value.
+ *   lanes_per_cand  {1,2,4,8,16}: lanes sharing one distance (both kernels)
+ *   visited_bits    [8, 13]: slots of the per-query visited cache (2^bits)
+ *   warps_per_block {1..16} and blocks_per_sm {1..32}: fast kernel shape
+ *                   (blocks_per_sm 0 = as many as fit)
+ *   mode            1: fast kernel for every query, heap kernel for the
+ *                   queries whose distances tie; 2: heap kernel for every
+ *                   query (best when ties are common, e.g. integer data)
+ *   heap_warps      {1..8}: warps per block of the heap kernel
+ *   heap_scap       [256, 16384]: search-pool slots per query in shared
+ *                   memory (larger pools go to the global-memory kernel) */
 typedef struct {
     uint32_t lanes_per_cand;
     uint32_t visited_bits;
     uint32_t warps_per_block;
     uint32_t blocks_per_sm;
+    uint32_t mode;
+    uint32_t heap_warps;
+    uint32_t heap_scap;
 } lqg_tuning;
 
 LQG_API lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t);

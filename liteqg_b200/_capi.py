@@ -31,7 +31,7 @@ SIGNATURES = {
     "lqg_set_arrays": (C.c_int, [_vp, C.c_uint32, _vp, _vp, _vp, _vp]),
     "lqg_get_arrays": (C.c_int, [_vp, _u32p, _vp, _vp, _vp, _vp]),
     "lqg_set_ef": (C.c_int, [_vp, C.c_uint32]),
-    "lqg_build": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64]),
+    "lqg_build": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32]),
     "lqg_search": (C.c_int, [_vp, _vp, C.c_uint32, _vp]),
     "lqg_search_batch_device": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
                                           _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
@@ -56,6 +56,9 @@ class Tuning(C.Structure):
         ("visited_bits", C.c_uint32),
         ("warps_per_block", C.c_uint32),
         ("blocks_per_sm", C.c_uint32),
+        ("mode", C.c_uint32),
+        ("heap_warps", C.c_uint32),
+        ("heap_scap", C.c_uint32),
     ]
 
 

@@ -370,10 +370,11 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     // barrier; kept marks go to s_keep, which the loop never reads; every
     // thread counts kept candidates in a register, so all threads take the
     // same branches.
+    const uint32_t cap = a.out_cap ? min(a.out_cap, a.deg) : a.deg;
     uint32_t kept_n = 0;
     for (uint32_t j = 0; j < P; ++j) {
         if (s_state[j] != 0) continue;
-        if (kept_n >= a.deg) break;
+        if (kept_n >= cap) break;
         ++kept_n;
         if (tid == 0) s_keep[j] = 1;
         for (uint32_t i = j + 1 + tid; i < P; i += kPruneThreads)
@@ -384,16 +385,16 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     if (tid == 0) {
         uint32_t* out = a.out + node * a.deg;
         uint32_t w = 0;
-        for (uint32_t j = 0; j < P && w < a.deg; ++j)
+        for (uint32_t j = 0; j < P && w < cap; ++j)
             if (s_keep[j]) out[w++] = s_ids[j];
         const uint32_t kept = w;
         if (a.fill)
-            for (uint32_t j = 0; j < P && w < a.deg; ++j)
+            for (uint32_t j = 0; j < P && w < cap; ++j)
                 if (!s_keep[j]) out[w++] = s_ids[j];
         if (a.rest_fill) {  // caller's earlier pruned list
             const uint32_t* rr = a.rest_fill + node * a.rest_stride;
             const uint32_t rc = min(a.rest_fill_cnt[node], a.rest_stride);
-            for (uint32_t j = 0; j < rc && w < a.deg; ++j) {
+            for (uint32_t j = 0; j < rc && w < cap; ++j) {
                 const uint32_t v = rr[j];
                 bool dup = v == (uint32_t)node;
                 for (uint32_t t = 0; t < w && !dup; ++t) dup = out[t] == v;

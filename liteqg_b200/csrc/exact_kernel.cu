@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(256) exact_search_kernel(SearchArgs a, ExactSc
                 heap_pop(rp, rn);
             }
             if (a.stats) {
-                uint4 st = make_uint4(pops, evals, 1u, P);
+                uint4 st = make_uint4(pops, evals, 2u, P);
                 *reinterpret_cast<uint4*>(a.stats + 4 * (size_t)qi) = st;
             }
         }

@@ -96,9 +96,12 @@ lqg_status ensure_ctl(Workspace& w, int64_t m) {
     }
     if (w.flagged_cap < m) {
         dfree(w.d_flagged);
+        dfree(w.d_spill);
         const int64_t cap = std::max<int64_t>(m, 1024);
-        if (cudaMalloc(&w.d_flagged, cap * sizeof(int32_t)) != cudaSuccess) {
+        if (cudaMalloc(&w.d_flagged, cap * sizeof(int32_t)) != cudaSuccess ||
+            cudaMalloc(&w.d_spill, cap * sizeof(int32_t)) != cudaSuccess) {
             cudaGetLastError();
+            dfree(w.d_flagged);
             w.flagged_cap = 0;
             return fail(LQG_ERR_NOMEM, "flag list allocation failed");
         }
@@ -197,31 +200,69 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     const int E = pool_regs_for(b.ef0);
     const int degw = (int)(ix->deg / 32);
     const lqg_tuning& t = ix->tune;
-    SearchArgs a = base_args(ix, w, b);
-    a.qhead = w.d_ctl + kCtlFastHead;
-    a.nflagged = w.d_ctl + kCtlFlagged;
-    a.flagged = w.d_flagged;
-    a.vbits = t.visited_bits;
-    a.ties_ok = b.ties_ok;
-    int warps = plain ? 1 : (int)t.warps_per_block;
-    int blocks = 1;
-    if (!plain) {
-        int occ = t.blocks_per_sm ? (int)t.blocks_per_sm
-                                  : lqg::fast_occupancy(E, (int)t.lanes_per_cand, degw, warps,
-                                                        ix->dim, t.visited_bits);
-        if (occ <= 0) return fail(LQG_ERR_ARG, "fast kernel cannot launch with this tuning");
-        blocks = occ * ix->num_sms;
-        const int64_t need = (b.m + warps - 1) / warps;
-        if (need < blocks) blocks = (int)need;
-    }
-    if (ix->ev_start) LQG_CUDA(cudaEventRecord(ix->ev_start, b.st));
-    cudaError_t e = lqg::launch_fast(a, E, (int)t.lanes_per_cand, degw, warps, blocks, b.st);
-    if (e != cudaSuccess) return cuda_fail(e, "fast search launch");
-    if (ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
+    const bool heap_all = t.mode == 2;
+    cudaError_t e;
 
+    // 1. fast kernel over every query (mode 1); tied queries go to the list
+    if (!heap_all) {
+        SearchArgs a = base_args(ix, w, b);
+        a.qhead = w.d_ctl + kCtlFastHead;
+        a.nflagged = w.d_ctl + kCtlFlagged;
+        a.flagged = w.d_flagged;
+        a.vbits = t.visited_bits;
+        a.ties_ok = b.ties_ok;
+        int warps = plain ? 1 : (int)t.warps_per_block;
+        int blocks = 1;
+        if (!plain) {
+            int occ = t.blocks_per_sm ? (int)t.blocks_per_sm
+                                      : lqg::fast_occupancy(E, (int)t.lanes_per_cand, degw, warps,
+                                                            ix->dim, t.visited_bits);
+            if (occ <= 0) return fail(LQG_ERR_ARG, "fast kernel cannot launch with this tuning");
+            blocks = occ * ix->num_sms;
+            const int64_t need = (b.m + warps - 1) / warps;
+            if (need < blocks) blocks = (int)need;
+        }
+        if (ix->ev_start) LQG_CUDA(cudaEventRecord(ix->ev_start, b.st));
+        e = lqg::launch_fast(a, E, (int)t.lanes_per_cand, degw, warps, blocks, b.st);
+        if (e != cudaSuccess) return cuda_fail(e, "fast search launch");
+        if (ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
+    }
+
+    // 2. heap kernel: the flagged queries (mode 1) or all of them (mode 2)
+    {
+        SearchArgs h = base_args(ix, w, b);
+        if (!heap_all) {
+            h.qlist = w.d_flagged;
+            h.nlist = w.d_ctl + kCtlFlagged;
+        }
+        h.qhead = w.d_ctl + kCtlHeapHead;
+        h.vbits = t.visited_bits;
+        lqg::HeapArgs hp{};
+        hp.rcap = (b.ef0 + 2u) & ~1u;
+        hp.scap = t.heap_scap;
+        hp.spill = w.d_spill;
+        hp.nspill = w.d_ctl + kCtlSpilled;
+        int hw = plain ? 1 : (int)t.heap_warps;
+        int hb = 1;
+        if (!plain) {
+            int occ = 0;
+            e = lqg::launch_heap(h, hp, (int)t.lanes_per_cand, degw, hw, 0, b.st, &occ);
+            if (e != cudaSuccess || occ <= 0)
+                return fail(LQG_ERR_ARG, "heap kernel cannot launch with this tuning");
+            hb = occ * ix->num_sms;
+            const int64_t need = (b.m + hw - 1) / hw;
+            if (need < hb) hb = (int)need;
+        }
+        if (heap_all && ix->ev_start) LQG_CUDA(cudaEventRecord(ix->ev_start, b.st));
+        e = lqg::launch_heap(h, hp, (int)t.lanes_per_cand, degw, hw, hb, b.st, nullptr);
+        if (e != cudaSuccess) return cuda_fail(e, "heap search launch");
+        if (heap_all && ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
+    }
+
+    // 3. exact global-memory kernel: queries whose search pool outgrew shared memory
     SearchArgs x = base_args(ix, w, b);
-    x.qlist = w.d_flagged;
-    x.nlist = w.d_ctl + kCtlFlagged;
+    x.qlist = w.d_spill;
+    x.nlist = w.d_ctl + kCtlSpilled;
     x.qhead = w.d_ctl + kCtlExactHead;
     int xb = plain ? 1 : w.x_blocks;
     int xw = plain ? 1 : w.x_warps_per_block;
@@ -549,6 +590,22 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         if (t->blocks_per_sm > 32) return fail(LQG_ERR_ARG, "blocks_per_sm must be <= 32");
         n.blocks_per_sm = t->blocks_per_sm;
     }
+    if (t->mode) {
+        if (t->mode > 2) return fail(LQG_ERR_ARG, "mode must be 1 or 2");
+        n.mode = t->mode;
+    }
+    if (t->heap_warps) {
+        if (t->heap_warps > 8) return fail(LQG_ERR_ARG, "heap_warps must be <= 8");
+        n.heap_warps = t->heap_warps;
+    }
+    if (t->heap_scap) {
+        if (t->heap_scap < 256 || t->heap_scap > 16384)
+            return fail(LQG_ERR_ARG, "heap_scap must be in [256, 16384]");
+        n.heap_scap = t->heap_scap;
+    }
+    if (lqg::heap_smem_bytes(ix->dim, n.visited_bits, kMaxEf + 2, n.heap_scap, (int)n.heap_warps) >
+        227 * 1024)
+        return fail(LQG_ERR_ARG, "heap kernel tuning needs more than 227 KB of shared memory");
     if (lqg::fast_smem_bytes(ix->dim, n.visited_bits, (int)n.warps_per_block) > 227 * 1024)
         return fail(LQG_ERR_ARG, "tuning needs more than 227 KB of shared memory per block");
     ix->tune = n;
@@ -595,11 +652,12 @@ lqg_status lqg_device_arrays(const lqg_index* ix, const uint32_t** nbrs, const u
 //              target's list re-pruned, then filled to exactly degree_bound
 //              with its pruned candidates and, if still short, random ids.
 lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32_t num_iter,
-                     uint64_t seed) {
+                     uint64_t seed, uint32_t random_edges) {
     if (!ix || !data) return fail(LQG_ERR_ARG, "null argument");
     if (num_iter <= 1) return fail(LQG_ERR_ARG, "The number of iter for building qg should >= 3");
     if (ef_build == 0 || ef_build > kMaxEf) return fail(LQG_ERR_ARG, "EF must be in [1, 512]");
     if (ix->n <= ix->deg) return fail(LQG_ERR_ARG, "num_elements must exceed degree_bound");
+    if (random_edges >= ix->deg) return fail(LQG_ERR_ARG, "random_edges must be below degree_bound");
     DeviceScope ds(ix->device);
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
     const uint64_t n = ix->n;
@@ -733,6 +791,7 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
         b.rev_cap = rev_cap;
         b.out = d_new;
         b.out_cnt = d_new_cnt;
+        b.out_cap = deg - random_edges;
         b.fill = 1;
         b.rest_fill = d_rest;
         b.rest_fill_cnt = d_rest_cnt;

@@ -26,6 +26,7 @@ struct PruneArgs {
     const uint32_t* rev_end;    // [n] segment end
     uint32_t rev_cap;           // sources taken per node (lowest ids first)
     // outputs
+    uint32_t out_cap;    // ids written per node at most (0 = deg)
     uint32_t* out;       // [n][deg]
     uint32_t* out_cnt;   // [n] ids written
     uint32_t* kept_cnt;  // [n] ids kept by the prune (or null)

@@ -32,7 +32,15 @@ void dfree(T*& p) {
 }
 
 // Control words in device memory, zeroed before every batch.
-enum : int { kCtlFastHead = 0, kCtlFlagged = 1, kCtlExactHead = 2, kCtlErr = 3, kCtlErrQuery = 4 };
+enum : int {
+    kCtlFastHead = 0,
+    kCtlFlagged = 1,
+    kCtlExactHead = 2,
+    kCtlErr = 3,
+    kCtlErrQuery = 4,
+    kCtlHeapHead = 5,
+    kCtlSpilled = 6
+};
 constexpr int kCtlWords = 8;
 
 constexpr uint32_t kMaxEf = 512;
@@ -43,7 +51,8 @@ constexpr uint32_t kMaxEf = 512;
 // each need their own.
 struct Workspace {
     uint32_t* d_ctl = nullptr;
-    int32_t* d_flagged = nullptr;
+    int32_t* d_flagged = nullptr;  // fast kernel -> heap kernel
+    int32_t* d_spill = nullptr;    // heap kernel -> exact kernel
     int64_t flagged_cap = 0;
     ExactScratch xs{};
     int x_blocks = 0, x_warps_per_block = 4;
@@ -59,6 +68,7 @@ struct Workspace {
     void release() {
         dfree(d_ctl);
         dfree(d_flagged);
+        dfree(d_spill);
         flagged_cap = 0;
         dfree(xs.vis);
         dfree(xs.sp);
@@ -145,7 +155,7 @@ struct lqg_index {
     lqg_host::Workspace ws;  // the default work area (one batch at a time)
 
     cudaStream_t own_stream = nullptr;
-    lqg_tuning tune{4, 10, 8, 0};
+    lqg_tuning tune{4, 10, 8, 0, 1, 4, 1024};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // recorded around the fast kernel
 
     ~lqg_index() {

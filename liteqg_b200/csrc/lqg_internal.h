@@ -22,4 +22,23 @@ cudaError_t launch_exact(const SearchArgs& a, const ExactScratch& s, int degw, i
                          int blocks, cudaStream_t st);
 size_t exact_smem_bytes(uint32_t dim, int warps);
 
+// Heap kernel: per-warp shared-memory capacities and the list of queries whose
+// search pool outgrew them (handed to the exact kernel).
+struct HeapArgs {
+    uint32_t rcap;      // result-pool slots (>= ef + 1)
+    uint32_t scap;      // search-pool slots
+    int32_t* spill;     // [m] queries that overflowed scap
+    uint32_t* nspill;
+};
+
+__host__ __device__ inline size_t heap_warp_bytes(uint32_t dim, uint32_t vbits, uint32_t rcap,
+                                                  uint32_t scap) {
+    const size_t dpad = (dim + 15u) & ~15u;
+    return 4 * dpad + 4 * ((size_t)1 << vbits) + kCandBytes + 8 * (size_t)rcap + 8 * (size_t)scap;
+}
+size_t heap_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t rcap, uint32_t scap, int warps);
+// Launches the heap kernel (or, with occ != null, only reports resident blocks per SM).
+cudaError_t launch_heap(const SearchArgs& a, const HeapArgs& h, int G, int degw, int warps,
+                        int blocks, cudaStream_t st, int* occ);
+
 }  // namespace lqg

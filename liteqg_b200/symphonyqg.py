@@ -86,8 +86,11 @@ class Index:
         check(lib().lqg_set_ef(self.handle, int(EF)))
 
     def build_index(self, data, EF: int, num_iter: int = 3, num_thread: int = UINT_MAX,
-                    seed: int = 0) -> None:
-        """Builds on the GPU (``num_thread`` is accepted and unused)."""
+                    seed: int = 0, random_edges: int | None = None) -> None:
+        """Builds on the GPU (``num_thread`` is accepted and unused).
+
+        ``random_edges`` slots of each neighbour list hold seeded random
+        long-range links (default ``degree_bound // 8``)."""
         items = _as_f32(data)
         if items.ndim == 1:
             items = items.reshape(1, -1)
@@ -97,7 +100,8 @@ class Index:
                 f"({self.num_elements}, {self.dimension}), but got: {tuple(items.shape)}")
         if num_iter <= 1:
             raise ValueError("The number of iter for building qg should >= 3")
-        check(lib().lqg_build(self.handle, _p(items), int(EF), int(num_iter), int(seed)))
+        re = self.degree_bound // 8 if random_edges is None else int(random_edges)
+        check(lib().lqg_build(self.handle, _p(items), int(EF), int(num_iter), int(seed), re))
 
     def search(self, query, k: int, ef=None, return_pool: bool = False,
                return_stats: bool = False):
@@ -185,8 +189,9 @@ class Index:
         return int(e.value), v, nb, cd, pr
 
     def set_tuning(self, lanes_per_cand=0, visited_bits=0, warps_per_block=0,
-                   blocks_per_sm=0) -> None:
-        t = Tuning(lanes_per_cand, visited_bits, warps_per_block, blocks_per_sm)
+                   blocks_per_sm=0, mode=0, heap_warps=0, heap_scap=0) -> None:
+        t = Tuning(lanes_per_cand, visited_bits, warps_per_block, blocks_per_sm, mode,
+                   heap_warps, heap_scap)
         check(lib().lqg_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
