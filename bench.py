@@ -48,14 +48,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "QPS @ recall@10≥0.95: batched vs plain GPU vs CPU; p50/p99 ms; HBM GB/s"
-BUILDER_VERSION = "gpu-builder-1"
+BUILDER_VERSION = "gpu-builder-2"
 
 WORKLOADS = {
     "batched-1m128": dict(n=1_000_000, dim=128, gen="int_mixture", clusters=1024, lo=0.0,
-                          hi=255.0, sigma=20.0, deg=32, efb=400, iters=3, nq=10_000, k=10,
-                          efs=(64, 128, 256), k_extra=100),
-    "small-100k64": dict(n=100_000, dim=64, gen="uniform", deg=32, efb=200, iters=3, nq=1000,
-                         k=10, efs=(20, 40, 60, 100, 200), k_extra=100),
+                          hi=255.0, sigma=20.0, deg=32, efb=400, iters=3, random_edges=16,
+                          nq=10_000, k=10, efs=(64, 128, 256), k_extra=100),
+    "small-100k64": dict(n=100_000, dim=64, gen="uniform", deg=32, efb=200, iters=3,
+                         random_edges=4, nq=1000, k=10, efs=(20, 40, 60, 100, 200), k_extra=100),
 }
 
 
@@ -102,7 +102,7 @@ def get_index_file(name, w, base, device):
         return path, 0.0
     ix = liteqg_b200.Index("QG", "L2", w["n"], w["dim"], w["deg"], device=device)
     t = time.perf_counter()
-    ix.build_index(base, w["efb"], num_iter=w["iters"])
+    ix.build_index(base, w["efb"], num_iter=w["iters"], random_edges=w["random_edges"])
     tb = time.perf_counter() - t
     tmp = path + f".tmp{os.getpid()}"
     ix.save(tmp)
@@ -340,10 +340,26 @@ def gpu_arm(args, w, name, rank, world, device):
     stx = st.cpu().numpy().astype(np.int64)
     stf = st_fast.cpu().numpy().astype(np.int64)
     pops, evals = stx[:, 0], stx[:, 1]
-    exact_share = float((stf[:, 2] == 1).mean())
+    exact_share = float((stf[:, 2] >= 1).mean())
+    # launch shape and policy (fast+heap or heap-only, buffer sizes): autotuned
+    # on the first 4,000 queries; every setting gives the same ids
+    from liteqg_b200 import autotune
+
+    tuned = autotune.tune(ix, queries[:4000], chosen, k, path=None, device=device)
+    mode = tuned["mode"]
+    mode_ms = {str(c): t for t, c in tuned["all"]}
+    if args.profile:
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_push("lqg_profile")
+        for _ in range(args.profile):
+            ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=chosen, stream=sh)
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_pop()
+        ix.stream_status(sh)
+        log(f"[rank {rank}] profiled {args.profile} steps, mode {mode} {mode_ms}")
+        return
     # algorithmic bytes (per launch): neighbour rows of popped nodes, codes of
     # evaluated nodes (+ the entry), the query; SQ8 params once per CTA
-    tune = ix.get_tuning()
     bytes_launch = float((pops * 4 * deg + (evals + 1) * dim + 4 * dim).sum())
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -373,6 +389,7 @@ def gpu_arm(args, w, name, rank, world, device):
         torch.cuda.synchronize(dev)
     ix.set_kernel_events(0, 0)
     ix.stream_status(sh)
+    tune = ix.get_tuning()
     log(f"[rank {rank}] timed loop done {time.perf_counter() - t0:.1f}s")
     step_ms = [a.elapsed_time(b) for a, b in ev]
     kern_ms = [a.elapsed_time(b) for a, b in kev]
@@ -460,18 +477,20 @@ def gpu_arm(args, w, name, rank, world, device):
         "warmup": max(3, args.warmup), "ms_per_step": statistics.mean(step_ms),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']}, {nq} queries/GPU, "
+        "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']} "
+                               f"(random_edges={w['random_edges']}), {nq} queries/GPU, "
                                f"k={k}, ef={chosen}", "ef": chosen, "k": k,
                    "recall_at_10_pool": recall.get(chosen), "recall_by_ef": recall,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "tuning": tune, "exact_path_share": exact_share,
+                   "tuning": tune, "autotune_ms": mode_ms, "tied_query_share": exact_share,
                    "fast_vs_exact_id_mismatch": mismatch, "e2e_ids_equal": e2e_ok,
                    "pops_mean": float(pops.mean()), "evals_mean": float(evals.mean())},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic_launch, "algorithmic_bytes_per_launch": bytes_launch,
                      "kernel_ms": statistics.mean(kern_ms),
-                     "kernel": "fast_search_kernel"},
+                     "kernel": ("fast_search_kernel + heap_search_kernel (tied queries)" if mode == 1
+                                else "heap_search_kernel")},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": int(nq * dim * 4),
                 "d2h_bytes_per_step": int(nq * k * 4)},
         "gpu_launches": 2 * K,
@@ -493,6 +512,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched-1m128", choices=sorted(WORKLOADS))
+    ap.add_argument("--profile", type=int, default=0,
+                    help="run N batched steps inside an NVTX range 'lqg_profile' and exit")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -200,9 +200,9 @@ LQG_API lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t);
 LQG_API lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t);
 
 /* Profiling hook: when both are non-NULL cudaEvent_t handles, every later
- * batch records `start` just before and `stop` just after the fast search
- * kernel, on the batch's stream (NULL, NULL turns it off). The events stay
- * owned by the caller. */
+ * batch records `start` just before its first search kernel and `stop` just
+ * after its last, on the batch's stream (NULL, NULL turns it off). The events
+ * stay owned by the caller. */
 LQG_API lqg_status lqg_set_kernel_events(lqg_index* ix, void* start, void* stop);
 
 /* Basic properties. */

@@ -21,8 +21,9 @@
 // fails the acceptance test (any trimmed or rejected node is at or above the
 // current bound), or it is still in the result pool, which is checked before
 // it could be pushed twice. So the accepted sequence equals the reference's.
-// A query whose search pool outgrows the shared-memory capacity goes to the
-// global-memory exact kernel through a second list.
+// The search pool keeps its first scap slots in shared memory and the deeper
+// heap levels in a per-warp global-memory area; a query whose search pool
+// outgrows both goes to the global-memory exact kernel through a second list.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -37,57 +38,71 @@ __device__ __forceinline__ bool hless(uint2 x, uint2 y) {
     return __uint_as_float(x.y) < __uint_as_float(y.y);
 }
 
+// A heap array: slots [0, cap) in shared memory, slots >= cap (the deepest
+// levels of a large search pool) in a per-warp global-memory area.
+struct HeapView {
+    uint2* s;
+    uint2* g;
+    uint32_t cap;
+    __device__ __forceinline__ uint2 get(uint32_t i) const { return i < cap ? s[i] : g[i - cap]; }
+    __device__ __forceinline__ void set(uint32_t i, uint2 v) const {
+        if (i < cap)
+            s[i] = v;
+        else
+            g[i - cap] = v;
+    }
+};
+
 // Sift-up of v from slot `hole` (libstdc++ __push_heap with top 0), all lanes.
-__device__ __forceinline__ void warp_sift_up(uint2* h, uint32_t hole, uint2 v, int lane) {
+__device__ __forceinline__ void warp_sift_up(HeapView h, uint32_t hole, uint2 v, int lane) {
     // ancestors of hole: ((hole + 1) >> i) - 1 for i = 1 .. depth
     const uint32_t p1 = hole + 1;
     const uint32_t depth = 31u - __clz(p1);  // floor(log2(hole + 1))
     bool pred = false;
     uint2 anc = make_uint2(0, 0);
-    uint32_t ai = 0;
     if (lane >= 1 && (uint32_t)lane <= depth) {
-        ai = (p1 >> lane) - 1u;
-        anc = h[ai];
+        anc = h.get((p1 >> lane) - 1u);
         pred = hless(anc, v);
     }
     const unsigned m = __ballot_sync(kFull, pred);
-    // consecutive trues from level 1 upward
+    // consecutive trues from level 1 upward: the loop of __push_heap stops
+    // at the first parent that is not less than the value
     const uint32_t j = (uint32_t)(__ffs(~(m >> 1)) - 1);
     // level l (1..j): its value moves down to level l - 1
-    if (lane >= 1 && (uint32_t)lane <= j) h[(p1 >> (lane - 1)) - 1u] = anc;
-    if (lane == 0) h[(p1 >> j) - 1u] = v;
+    if (lane >= 1 && (uint32_t)lane <= j) h.set((p1 >> (lane - 1)) - 1u, anc);
+    if (lane == 0) h.set((p1 >> j) - 1u, v);
     __syncwarp();
 }
 
-__device__ __forceinline__ void warp_push(uint2* h, uint32_t& n, uint2 v, int lane) {
+__device__ __forceinline__ void warp_push(HeapView h, uint32_t& n, uint2 v, int lane) {
     warp_sift_up(h, n, v, lane);
     ++n;
 }
 
 // pop_heap + pop_back.
-__device__ __forceinline__ void warp_pop(uint2* h, uint32_t& n, int lane) {
+__device__ __forceinline__ void warp_pop(HeapView h, uint32_t& n, int lane) {
     const uint32_t size = n;
     if (size > 1) {
         uint32_t hole = 0;
         uint2 v = make_uint2(0, 0);
         if (lane == 0) {
             const uint32_t len = size - 1;
-            v = h[len];
+            v = h.get(len);
             uint32_t second = 0;
             while (second < (len - 1) / 2) {
                 second = 2 * (second + 1);
-                const uint2 r = h[second], l = h[second - 1];
+                const uint2 r = h.get(second), l = h.get(second - 1);
                 if (hless(r, l)) {
                     second--;
-                    h[hole] = l;
+                    h.set(hole, l);
                 } else {
-                    h[hole] = r;
+                    h.set(hole, r);
                 }
                 hole = second;
             }
             if ((len & 1u) == 0 && second == (len - 2) / 2) {
                 second = 2 * (second + 1);
-                h[hole] = h[second - 1];
+                h.set(hole, h.get(second - 1));
                 hole = second - 1;
             }
         }
@@ -103,7 +118,7 @@ __device__ __forceinline__ void warp_pop(uint2* h, uint32_t& n, int lane) {
 }  // namespace
 
 template <int G, int DEGW>
-__global__ void __launch_bounds__(256) heap_search_kernel(SearchArgs a, HeapArgs hp) {
+__global__ void __launch_bounds__(256, 1) heap_search_kernel(SearchArgs a, HeapArgs hp) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -118,8 +133,11 @@ __global__ void __launch_bounds__(256) heap_search_kernel(SearchArgs a, HeapArgs
     uint32_t* vis = reinterpret_cast<uint32_t*>(wb + 4u * dpad);
     uint32_t* cid = vis + vsize;
     float* cd = reinterpret_cast<float*>(cid + kMaxDeg);
-    uint2* rp = reinterpret_cast<uint2*>(cd + kMaxDeg);
-    uint2* sp = rp + hp.rcap;
+    uint2* rps = reinterpret_cast<uint2*>(cd + kMaxDeg);
+    const HeapView rp{rps, nullptr, hp.rcap};
+    const size_t gw = (size_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    const HeapView sp{rps + hp.rcap, hp.sp_global + gw * hp.gcap, hp.scap};
+    const uint32_t sp_max = hp.scap + hp.gcap;
 
     for (uint32_t i = threadIdx.x; i < dpad; i += blockDim.x) {
         pmin[i] = i < dim ? a.params[2 * i] : 0.f;
@@ -153,8 +171,8 @@ __global__ void __launch_bounds__(256) heap_search_kernel(SearchArgs a, HeapArgs
         d0 = __shfl_sync(kFull, d0, 0);
         uint32_t sn = 0, rn = 0;
         if (lane == 0) {
-            sp[0] = make_uint2(ep, __float_as_uint(-d0));
-            rp[0] = make_uint2(ep, __float_as_uint(d0));
+            sp.set(0, make_uint2(ep, __float_as_uint(-d0)));
+            rp.set(0, make_uint2(ep, __float_as_uint(d0)));
             vis[hash_id(ep, vbits)] = ep;
         }
         sn = 1;
@@ -167,7 +185,7 @@ __global__ void __launch_bounds__(256) heap_search_kernel(SearchArgs a, HeapArgs
         for (;;) {
             // qg.hpp:313-318
             if (sn == 0) break;
-            const uint2 top = sp[0];
+            const uint2 top = sp.get(0);
             if (-__uint_as_float(top.y) > lower) break;
             warp_pop(sp, sn, lane);
             const uint32_t u = top.x;
@@ -226,16 +244,16 @@ __global__ void __launch_bounds__(256) heap_search_kernel(SearchArgs a, HeapArgs
                     if (!(rn < ef || lower > y)) continue;
                     // a forgotten, already pooled node: the reference has it visited
                     bool in_rp = false;
-                    for (uint32_t i = lane; i < rn; i += 32) in_rp |= rp[i].x == id;
+                    for (uint32_t i = lane; i < rn; i += 32) in_rp |= rps[i].x == id;
                     if (__any_sync(kFull, in_rp)) continue;
-                    if (sn + 1 > hp.scap) {
+                    if (sn + 1 > sp_max) {
                         overflow = true;
                         break;
                     }
                     warp_push(sp, sn, make_uint2(id, __float_as_uint(-y)), lane);
                     warp_push(rp, rn, make_uint2(id, __float_as_uint(y)), lane);
                     if (rn > ef) warp_pop(rp, rn, lane);
-                    lower = __uint_as_float(rp[0].y);
+                    lower = __uint_as_float(rps[0].y);
                 }
                 if (overflow) break;
             }
@@ -261,7 +279,7 @@ __global__ void __launch_bounds__(256) heap_search_kernel(SearchArgs a, HeapArgs
                 a.pool_d[(size_t)qi * a.pstride + j] = CUDART_INF_F;
             }
         for (uint32_t j = 0; rn > 0; ++j) {
-            const uint2 t = rp[0];
+            const uint2 t = rps[0];
             if (lane == 0) {
                 if (j < k) out[k - 1 - j] = t.x;
                 const uint32_t pos = P - 1 - j;

@@ -225,7 +225,6 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         if (ix->ev_start) LQG_CUDA(cudaEventRecord(ix->ev_start, b.st));
         e = lqg::launch_fast(a, E, (int)t.lanes_per_cand, degw, warps, blocks, b.st);
         if (e != cudaSuccess) return cuda_fail(e, "fast search launch");
-        if (ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
     }
 
     // 2. heap kernel: the flagged queries (mode 1) or all of them (mode 2)
@@ -253,10 +252,21 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             const int64_t need = (b.m + hw - 1) / hw;
             if (need < hb) hb = (int)need;
         }
+        const size_t slots = (size_t)hb * hw;
+        if (w.sp_global_slots < slots) {
+            dfree(w.d_sp_global);
+            w.sp_global_slots = 0;
+            if (cudaMalloc(&w.d_sp_global, slots * kHeapGlobalCap * sizeof(uint2)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(LQG_ERR_NOMEM, "heap kernel search-pool area allocation failed");
+            }
+            w.sp_global_slots = slots;
+        }
+        hp.sp_global = w.d_sp_global;
+        hp.gcap = kHeapGlobalCap;
         if (heap_all && ix->ev_start) LQG_CUDA(cudaEventRecord(ix->ev_start, b.st));
         e = lqg::launch_heap(h, hp, (int)t.lanes_per_cand, degw, hw, hb, b.st, nullptr);
         if (e != cudaSuccess) return cuda_fail(e, "heap search launch");
-        if (heap_all && ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
     }
 
     // 3. exact global-memory kernel: queries whose search pool outgrew shared memory
@@ -268,6 +278,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     int xw = plain ? 1 : w.x_warps_per_block;
     e = lqg::launch_exact(x, w.xs, degw, xw, xb, b.st);
     if (e != cudaSuccess) return cuda_fail(e, "exact search launch");
+    if (ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
     return LQG_OK;
 }
 

@@ -44,6 +44,7 @@ enum : int {
 constexpr int kCtlWords = 8;
 
 constexpr uint32_t kMaxEf = 512;
+constexpr uint32_t kHeapGlobalCap = 28672;  // heap kernel search-pool slots in global memory
 
 // Mutable device state of one batch in flight: control words, the list of
 // tie-flagged queries, the exact kernel's work areas, and staging buffers for
@@ -55,6 +56,8 @@ struct Workspace {
     int32_t* d_spill = nullptr;    // heap kernel -> exact kernel
     int64_t flagged_cap = 0;
     ExactScratch xs{};
+    uint2* d_sp_global = nullptr;  // heap kernel: search-pool slots beyond shared memory
+    size_t sp_global_slots = 0;    // warps covered
     int x_blocks = 0, x_warps_per_block = 4;
     float* d_q = nullptr;
     uint32_t* d_kq = nullptr;
@@ -73,6 +76,8 @@ struct Workspace {
         dfree(xs.vis);
         dfree(xs.sp);
         dfree(xs.rp);
+        dfree(d_sp_global);
+        sp_global_slots = 0;
         dfree(d_q);
         dfree(d_kq);
         dfree(d_efq);

@@ -25,9 +25,11 @@ size_t exact_smem_bytes(uint32_t dim, int warps);
 // Heap kernel: per-warp shared-memory capacities and the list of queries whose
 // search pool outgrew them (handed to the exact kernel).
 struct HeapArgs {
-    uint32_t rcap;      // result-pool slots (>= ef + 1)
-    uint32_t scap;      // search-pool slots
-    int32_t* spill;     // [m] queries that overflowed scap
+    uint32_t rcap;       // result-pool slots (>= ef + 1), shared memory
+    uint32_t scap;       // search-pool slots in shared memory
+    uint2* sp_global;    // [warps][gcap] further search-pool slots
+    uint32_t gcap;
+    int32_t* spill;      // [m] queries whose search pool outgrew scap + gcap
     uint32_t* nspill;
 };
 
