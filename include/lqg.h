@@ -199,6 +199,53 @@ typedef struct {
 LQG_API lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t);
 LQG_API lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t);
 
+/* ---- Serving loop (no reference counterpart) ----------------------------
+ * Continuous batching of single-query requests over one resident index: a
+ * dispatcher launches whatever is pending as one batch as soon as one of
+ * `streams` contexts is free, so requests that arrive while other batches
+ * are on the GPU are admitted as contexts free up and overlap with them.
+ * Each context holds the device state of at most `max_batch` requests
+ * (query, k, ef, ids, plus its own work areas); max_batch defaults to what
+ * `state_budget` bytes (default 256 MiB) allow. Results are exactly those of
+ * a search of the query alone. While a server runs, use the index only
+ * through it. */
+typedef struct lqg_server lqg_server;
+typedef struct {
+    uint32_t streams;      /* contexts (batches in flight), default 4 */
+    uint32_t max_batch;    /* requests per batch, default from state_budget */
+    uint64_t state_budget; /* device bytes for admitted requests, default 256 MiB */
+    uint32_t max_k;        /* largest k of a request, default 100 */
+    uint32_t max_ef;       /* largest ef of a request, default 512 */
+} lqg_server_config;
+typedef struct {
+    uint64_t completed;    /* requests finished since start / reset */
+    uint64_t batches;
+    double mean_batch;
+    double p50_us, p99_us; /* latency submit -> result */
+    double qps;            /* completed / elapsed */
+    uint32_t max_batch, streams;
+} lqg_server_metrics;
+
+LQG_API lqg_status lqg_server_start(lqg_index* ix, const lqg_server_config* cfg,
+                                    lqg_server** out);
+/* Copies `query` (D floats, host) and queues it; ef 0 = the index's set_ef. */
+LQG_API lqg_status lqg_server_submit(lqg_server* s, const float* query, uint32_t k,
+                                     uint32_t ef, uint64_t* ticket);
+/* Waits for a ticket (timeout_us < 0: forever), copies its k ids, releases it. */
+LQG_API lqg_status lqg_server_wait(lqg_server* s, uint64_t ticket, uint32_t* ids,
+                                   int64_t timeout_us, double* latency_us);
+/* Open-loop driver: submits query i at arrival_us[i] (from the call's start;
+ * NULL = as fast as possible) from a client thread, waits for all; ids
+ * [m][kstride], latency_us [m] (may be NULL). */
+LQG_API lqg_status lqg_server_replay(lqg_server* s, const float* queries, int64_t m,
+                                     const uint32_t* k, const uint32_t* ef,
+                                     const double* arrival_us, uint32_t* ids,
+                                     uint32_t kstride, double* latency_us);
+LQG_API lqg_status lqg_server_stats(lqg_server* s, lqg_server_metrics* out);
+LQG_API lqg_status lqg_server_reset_stats(lqg_server* s);
+/* Finishes queued requests, stops the threads, frees the contexts. */
+LQG_API lqg_status lqg_server_stop(lqg_server* s);
+
 /* Profiling hook: when both are non-NULL cudaEvent_t handles, every later
  * batch records `start` just before its first search kernel and `stop` just
  * after its last, on the batch's stream (NULL, NULL turns it off). The events

@@ -43,6 +43,13 @@ SIGNATURES = {
     "lqg_search_exact_noalloc": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
                                            _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
     "lqg_set_kernel_events": (C.c_int, [_vp, _vp, _vp]),
+    "lqg_server_start": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
+    "lqg_server_submit": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "lqg_server_wait": (C.c_int, [_vp, C.c_uint64, _vp, C.c_int64, C.POINTER(C.c_double)]),
+    "lqg_server_replay": (C.c_int, [_vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, C.c_uint32, _vp]),
+    "lqg_server_stats": (C.c_int, [_vp, _vp]),
+    "lqg_server_reset_stats": (C.c_int, [_vp]),
+    "lqg_server_stop": (C.c_int, [_vp]),
     "lqg_set_tuning": (C.c_int, [_vp, _vp]),
     "lqg_get_tuning": (C.c_int, [_vp, _vp]),
     "lqg_info": (C.c_int, [_vp, C.POINTER(C.c_uint64), _u32p, _u32p, _u32p, _u32p]),
@@ -59,6 +66,29 @@ class Tuning(C.Structure):
         ("mode", C.c_uint32),
         ("heap_warps", C.c_uint32),
         ("heap_scap", C.c_uint32),
+    ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("streams", C.c_uint32),
+        ("max_batch", C.c_uint32),
+        ("state_budget", C.c_uint64),
+        ("max_k", C.c_uint32),
+        ("max_ef", C.c_uint32),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_uint64),
+        ("batches", C.c_uint64),
+        ("mean_batch", C.c_double),
+        ("p50_us", C.c_double),
+        ("p99_us", C.c_double),
+        ("qps", C.c_double),
+        ("max_batch", C.c_uint32),
+        ("streams", C.c_uint32),
     ]
 
 
