@@ -182,10 +182,14 @@ LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
  *                   (blocks_per_sm 0 = as many as fit)
  *   mode            1: fast kernel for every query, heap kernel for the
  *                   queries whose distances tie; 2: heap kernel for every
- *                   query (best when ties are common, e.g. integer data)
+ *                   query; 3: replay kernel for every query (sorted-pool
+ *                   search warps, heap replay lanes; exact under ties)
  *   heap_warps      {1..8}: warps per block of the heap kernel
  *   heap_scap       [256, 16384]: search-pool slots per query in shared
- *                   memory (larger pools go to the global-memory kernel) */
+ *                   memory (heap and replay kernels; larger pools spill to
+ *                   global memory, then to the global-memory kernel)
+ *   replay_warps    {1..14}: search warps per block of the replay kernel
+ *                   (plus two replay warps) */
 typedef struct {
     uint32_t lanes_per_cand;
     uint32_t visited_bits;
@@ -194,6 +198,7 @@ typedef struct {
     uint32_t mode;
     uint32_t heap_warps;
     uint32_t heap_scap;
+    uint32_t replay_warps;
 } lqg_tuning;
 
 LQG_API lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t);

@@ -66,6 +66,7 @@ class Tuning(C.Structure):
         ("mode", C.c_uint32),
         ("heap_warps", C.c_uint32),
         ("heap_scap", C.c_uint32),
+        ("replay_warps", C.c_uint32),
     ]
 
 

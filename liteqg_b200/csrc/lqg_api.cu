@@ -99,7 +99,7 @@ lqg_status ensure_ctl(Workspace& w, int64_t m) {
         dfree(w.d_spill);
         const int64_t cap = std::max<int64_t>(m, 1024);
         if (cudaMalloc(&w.d_flagged, cap * sizeof(int32_t)) != cudaSuccess ||
-            cudaMalloc(&w.d_spill, cap * sizeof(int32_t)) != cudaSuccess) {
+            cudaMalloc(&w.d_spill, 2 * cap * sizeof(int32_t)) != cudaSuccess) {
             cudaGetLastError();
             dfree(w.d_flagged);
             w.flagged_cap = 0;
@@ -203,6 +203,50 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     const bool heap_all = t.mode == 2;
     cudaError_t e;
 
+    if (t.mode == 3) {
+        // replay kernel over every query; spilled queries go to the exact kernel
+        const int RE = lqg::replay_pool_regs(b.ef0);
+        if (RE == 0) return fail(LQG_ERR_ARG, "ef too large for the replay kernel");
+        SearchArgs h = base_args(ix, w, b);
+        h.qhead = w.d_ctl + kCtlHeapHead;
+        h.vbits = t.visited_bits;
+        lqg::ReplayArgs ra{};
+        ra.rcap = (b.ef0 + 2u) & ~1u;
+        ra.scap = t.heap_scap;
+        ra.spill = w.d_spill;
+        ra.nspill = w.d_ctl + kCtlSpilled;
+        int sw = plain ? 1 : (int)t.replay_warps;
+        while (sw > 1 && lqg::replay_smem_bytes(ix->dim, t.visited_bits, ra.rcap, ra.scap, sw) >
+                             227 * 1024)
+            --sw;
+        ra.swarps = (uint32_t)sw;
+        int rb = 1;
+        if (!plain) {
+            int occ = 0;
+            e = lqg::launch_replay(h, ra, RE, (int)t.lanes_per_cand, degw, 0, b.st, &occ);
+            if (e != cudaSuccess || occ <= 0)
+                return fail(LQG_ERR_ARG, "replay kernel cannot launch with this tuning");
+            rb = occ * ix->num_sms;
+            const int64_t need = (b.m + sw - 1) / sw;
+            if (need < rb) rb = (int)need;
+        }
+        const size_t slots = (size_t)rb * sw;
+        if (w.sp_global_slots < slots) {
+            dfree(w.d_sp_global);
+            w.sp_global_slots = 0;
+            if (cudaMalloc(&w.d_sp_global, slots * kHeapGlobalCap * sizeof(uint2)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(LQG_ERR_NOMEM, "replay kernel search-pool area allocation failed");
+            }
+            w.sp_global_slots = slots;
+        }
+        ra.sp_global = w.d_sp_global;
+        ra.gcap = kHeapGlobalCap;
+        if (ix->ev_start) LQG_CUDA(cudaEventRecord(ix->ev_start, b.st));
+        e = lqg::launch_replay(h, ra, RE, (int)t.lanes_per_cand, degw, rb, b.st, nullptr);
+        if (e != cudaSuccess) return cuda_fail(e, "replay search launch");
+    } else {
+
     // 1. fast kernel over every query (mode 1); tied queries go to the list
     if (!heap_all) {
         SearchArgs a = base_args(ix, w, b);
@@ -268,6 +312,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         e = lqg::launch_heap(h, hp, (int)t.lanes_per_cand, degw, hw, hb, b.st, nullptr);
         if (e != cudaSuccess) return cuda_fail(e, "heap search launch");
     }
+    }
 
     // 3. exact global-memory kernel: queries whose search pool outgrew shared memory
     SearchArgs x = base_args(ix, w, b);
@@ -291,6 +336,8 @@ lqg_status read_status(Workspace& w, cudaStream_t st) {
         if (ctl[kCtlErr] & lqg::kErrVisitedFull) why += " visited set full (32768 nodes);";
         if (ctl[kCtlErr] & lqg::kErrHeapFull) why += " search heap full (32768 entries);";
         if (ctl[kCtlErr] & lqg::kErrProbe) why += " visited-set probe failed;";
+        if (ctl[kCtlErr] & lqg::kErrSync)
+            return fail(LQG_ERR_CUDA, "replay kernel: a wait between its warps timed out");
         return fail(LQG_ERR_CAPACITY, "exact search work area overflow for query " +
                                           std::to_string(ctl[kCtlErrQuery]) + ":" + why);
     }
@@ -602,7 +649,7 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         n.blocks_per_sm = t->blocks_per_sm;
     }
     if (t->mode) {
-        if (t->mode > 2) return fail(LQG_ERR_ARG, "mode must be 1 or 2");
+        if (t->mode > 3) return fail(LQG_ERR_ARG, "mode must be 1, 2 or 3");
         n.mode = t->mode;
     }
     if (t->heap_warps) {
@@ -614,10 +661,19 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
             return fail(LQG_ERR_ARG, "heap_scap must be in [256, 16384]");
         n.heap_scap = t->heap_scap;
     }
-    if (lqg::heap_smem_bytes(ix->dim, n.visited_bits, kMaxEf + 2, n.heap_scap, (int)n.heap_warps) >
+    if (t->replay_warps) {
+        if (t->replay_warps > 14) return fail(LQG_ERR_ARG, "replay_warps must be in [1, 14]");
+        n.replay_warps = t->replay_warps;
+    }
+    if (n.mode == 3 &&
+        lqg::replay_smem_bytes(ix->dim, n.visited_bits, kMaxEf + 2, n.heap_scap, 1) > 227 * 1024)
+        return fail(LQG_ERR_ARG, "replay kernel tuning needs more than 227 KB of shared memory");
+    if (n.mode != 3 &&
+        lqg::heap_smem_bytes(ix->dim, n.visited_bits, kMaxEf + 2, n.heap_scap, (int)n.heap_warps) >
         227 * 1024)
         return fail(LQG_ERR_ARG, "heap kernel tuning needs more than 227 KB of shared memory");
-    if (lqg::fast_smem_bytes(ix->dim, n.visited_bits, (int)n.warps_per_block) > 227 * 1024)
+    if (n.mode == 1 &&
+        lqg::fast_smem_bytes(ix->dim, n.visited_bits, (int)n.warps_per_block) > 227 * 1024)
         return fail(LQG_ERR_ARG, "tuning needs more than 227 KB of shared memory per block");
     ix->tune = n;
     return LQG_OK;

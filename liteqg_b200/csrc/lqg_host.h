@@ -53,7 +53,7 @@ constexpr uint32_t kHeapGlobalCap = 28672;  // heap kernel search-pool slots in 
 struct Workspace {
     uint32_t* d_ctl = nullptr;
     int32_t* d_flagged = nullptr;  // fast kernel -> heap kernel
-    int32_t* d_spill = nullptr;    // heap kernel -> exact kernel
+    int32_t* d_spill = nullptr;    // heap/replay kernel -> exact kernel (2 x flagged_cap)
     int64_t flagged_cap = 0;
     ExactScratch xs{};
     uint2* d_sp_global = nullptr;  // heap kernel: search-pool slots beyond shared memory
@@ -160,7 +160,7 @@ struct lqg_index {
     lqg_host::Workspace ws;  // the default work area (one batch at a time)
 
     cudaStream_t own_stream = nullptr;
-    lqg_tuning tune{4, 10, 8, 0, 1, 4, 1024};
+    lqg_tuning tune{4, 10, 8, 0, 1, 4, 1024, 14};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // recorded around the fast kernel
 
     ~lqg_index() {

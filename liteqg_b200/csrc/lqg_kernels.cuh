@@ -68,6 +68,7 @@ enum : uint32_t {
     kErrVisitedFull = 1u,
     kErrHeapFull = 2u,
     kErrProbe = 4u,
+    kErrSync = 8u,  // replay kernel: a bounded wait between its warps ran out
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {

@@ -189,9 +189,10 @@ class Index:
         return int(e.value), v, nb, cd, pr
 
     def set_tuning(self, lanes_per_cand=0, visited_bits=0, warps_per_block=0,
-                   blocks_per_sm=0, mode=0, heap_warps=0, heap_scap=0) -> None:
+                   blocks_per_sm=0, mode=0, heap_warps=0, heap_scap=0,
+                   replay_warps=0) -> None:
         t = Tuning(lanes_per_cand, visited_bits, warps_per_block, blocks_per_sm, mode,
-                   heap_warps, heap_scap)
+                   heap_warps, heap_scap, replay_warps)
         check(lib().lqg_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:

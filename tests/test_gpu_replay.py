@@ -1,0 +1,163 @@
+"""GPU parity of the replay kernel (tuning mode 3) through the C ABI.
+
+Search warps run the sorted-pool form of the reference's loop and log every
+pool operation; replay lanes run the reference's two libstdc++ heaps from the
+log, check each step, and answer the search warps when equal distances make
+the heap layout decide. Bar: ids, FP32 pools and pop counts bit-exact against
+the reference's golden outputs and the oracle; queries only reach the exact
+global-memory kernel (stats flag 2) when a pool outgrows its capacity.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import SENTINEL, IndexArrays, Oracle, read_index, write_index
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lqg():
+    import liteqg_b200
+
+    return liteqg_b200
+
+
+def open_index(lqg, g, **tune):
+    ix = lqg.Index("QG", "L2", g["n"], g["dim"], g["deg"])
+    ix.load(g["path"])
+    ix.set_tuning(mode=3, **tune)
+    return ix
+
+
+def _oracle_for(g):
+    return Oracle(read_index(g["path"], g["n"], g["dim"], g["deg"]))
+
+
+def test_replay_golden_every_ef_k(lqg, golden):
+    """The reference's own outputs, every (ef, k) of the fixtures, batched and single."""
+    for name, g in golden.items():
+        ix = open_index(lqg, g)
+        for (ef, k), want in g["expected"].items():
+            ix.set_ef(ef)
+            got = ix.search(g["queries"], k)
+            assert np.array_equal(got, want), (name, ef, k)
+            one = ix.search(g["queries"][3], k)
+            assert np.array_equal(one, want[3]), (name, ef, k)
+
+
+def test_replay_pools_and_pops_bit_exact(lqg, golden):
+    for name, g in golden.items():
+        ix = open_index(lqg, g)
+        o = _oracle_for(g)
+        for ef in (10, 33, 100, 200, 480):
+            want = o.search(g["queries"], 10, ef)
+            ids, (pid, pd), st = ix.search(g["queries"], 10, ef=ef, return_pool=True,
+                                           return_stats=True)
+            assert np.array_equal(ids, want.compat), (name, ef)
+            for i in range(len(ids)):
+                p = want.pool_n[i]
+                assert st[i, 3] == p, (name, ef, i)
+                assert np.array_equal(pid[i, :p], want.pool_ids[i, :p]), (name, ef, i)
+                assert np.array_equal(pd[i, :p], want.pool_d[i, :p]), (name, ef, i)
+                assert (pid[i, p:] == SENTINEL).all()
+                assert st[i, 0] == want.pops[i], (name, ef, i)
+                assert st[i, 1] >= want.evals[i] + (0 if st[i, 2] == 2 else 1)
+            if name != "bin40":
+                # no pool outgrew its capacity: every query stayed in the replay kernel
+                assert (st[:, 2] == 0).all(), (name, ef, int((st[:, 2] != 0).sum()))
+
+
+@pytest.mark.parametrize("g_lanes,vbits,swarps,scap", [
+    (4, 10, 14, 512), (2, 8, 4, 256), (8, 13, 1, 2048), (4, 9, 7, 1024), (2, 12, 14, 256)])
+def test_replay_tuning_does_not_change_results(lqg, golden, g_lanes, vbits, swarps, scap):
+    for name in ("mix128d64", "bin40"):
+        g = golden[name]
+        ix = open_index(lqg, g, lanes_per_cand=g_lanes, visited_bits=vbits,
+                        replay_warps=swarps, heap_scap=scap)
+        for ef, k in ((20, 10), (50, 50), (200, 10)):
+            ix.set_ef(ef)
+            assert np.array_equal(ix.search(g["queries"], k), g["expected"][(ef, k)]), (name, ef, k)
+
+
+def test_replay_tie_heavy_binary_vectors(lqg, golden):
+    """Binary vectors: every query meets equal distances at the pop and the bound."""
+    g = golden["bin40"]
+    ix = open_index(lqg, g)
+    o = _oracle_for(g)
+    for ef in (20, 100, 200):
+        want = o.search(g["queries"], 50, ef)
+        ids, (pid, pd), st = ix.search(g["queries"], 50, ef=ef, return_pool=True,
+                                       return_stats=True)
+        assert np.array_equal(ids, want.compat), ef
+        assert np.array_equal(pd, want.pool_d), ef
+        assert np.array_equal(pid, want.pool_ids), ef
+        assert np.array_equal(st[:, 0], want.pops), ef
+
+
+def _device(ix, q, ef, k, kq=None, efq=None):
+    import torch
+
+    qt = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    m = qt.shape[0]
+    ids = torch.full((m, k), -1, dtype=torch.int32, device="cuda")
+    st = torch.zeros((m, 4), dtype=torch.int32, device="cuda")
+    kt = torch.from_numpy(kq).cuda() if kq is not None else None
+    et = torch.from_numpy(efq).cuda() if efq is not None else None
+    s = torch.cuda.current_stream()
+    ix.search_device(qt.data_ptr(), m, k, ids.data_ptr(), k, ef=ef,
+                     ef_ptr=et.data_ptr() if et is not None else 0,
+                     k_ptr=kt.data_ptr() if kt is not None else 0,
+                     stats_ptr=st.data_ptr(), stream=s.cuda_stream)
+    ix.stream_status(s.cuda_stream)
+    return ids.cpu().numpy().view(np.uint32), st.cpu().numpy()
+
+
+def _knn_graph(x, deg):
+    sq = (x.astype(np.float64) ** 2).sum(1)
+    n = len(x)
+    nb = np.empty((n, deg), np.uint32)
+    for s in range(0, n, 2048):
+        d = sq[s:s + 2048, None] + sq[None, :] - 2 * x[s:s + 2048].astype(np.float64) @ x.T.astype(np.float64)
+        d[np.arange(d.shape[0]), np.arange(s, s + d.shape[0])] = np.inf
+        nb[s:s + 2048] = np.argpartition(d, deg, axis=1)[:, :deg]
+    return nb
+
+
+@pytest.mark.parametrize("dim,deg,integer", [(128, 32, True), (96, 64, True), (64, 32, False)])
+def test_replay_larger_index_uneven_batch(lqg, tmp_path, dim, deg, integer):
+    """12k nodes, exact-kNN graph; per-query ef in {1..512} and k in {1, 10, 100}."""
+    from oracle.oracle import sq8_quantize
+
+    rng = np.random.default_rng(dim + deg)
+    n = 12000
+    if integer:
+        cent = rng.uniform(0, 255, (64, dim))
+        gen = lambda m: np.clip(np.rint(cent[rng.integers(0, 64, m)] + rng.normal(0, 20, (m, dim))),
+                                0, 255).astype(np.float32)
+    else:
+        gen = lambda m: rng.random((m, dim), dtype=np.float32)
+    x = gen(n)
+    codes, params = sq8_quantize(x, 2)
+    arr = IndexArrays(n, dim, deg, int(rng.integers(0, n)), x, _knn_graph(x, deg), codes, params)
+    path = str(tmp_path / "big.idx")
+    write_index(path, arr)
+    ix = lqg.Index("QG", "L2", n, dim, deg)
+    ix.load(path)
+    ix.set_tuning(mode=3)
+    o = Oracle(arr)
+    q = gen(400)
+    efq = rng.choice([1, 7, 32, 64, 100, 256, 512], size=len(q)).astype(np.uint32)
+    kq = rng.choice([1, 10, 100], size=len(q)).astype(np.uint32)
+    ids, st = _device(ix, q, 512, 100, kq=kq, efq=efq)
+    want = o.search(q, kq.astype(np.int32), efq.astype(np.int32))
+    for i in range(len(q)):
+        k = int(kq[i])
+        assert np.array_equal(ids[i, :k], want.compat[i, :k]), (i, efq[i], k)
+    assert np.array_equal(st[:, 0], want.pops)
+    assert (st[:, 2] == 0).mean() > 0.95, int((st[:, 2] != 0).sum())
+    for ef, k in ((64, 10), (256, 100)):
+        w = o.search(q, k, ef)
+        got, (pid, pd) = ix.search(q, k, ef=ef, return_pool=True)
+        assert np.array_equal(got, w.compat), (ef, k)
+        assert np.array_equal(pd, w.pool_d), (ef, k)
+        assert np.array_equal(pid, w.pool_ids), (ef, k)
