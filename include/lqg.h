@@ -188,8 +188,8 @@ LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
  *   heap_scap       [256, 16384]: search-pool slots per query in shared
  *                   memory (heap and replay kernels; larger pools spill to
  *                   global memory, then to the global-memory kernel)
- *   replay_warps    {1..14}: search warps per block of the replay kernel
- *                   (plus two replay warps) */
+ *   replay_warps    {1..15}: search warps per block of the replay kernel
+ *                   (plus one replay warp) */
 typedef struct {
     uint32_t lanes_per_cand;
     uint32_t visited_bits;

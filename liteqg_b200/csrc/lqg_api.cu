@@ -204,22 +204,30 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     cudaError_t e;
 
     if (t.mode == 3) {
-        // replay kernel over every query; spilled queries go to the exact kernel
+        // replay kernels over every query, in chunks whose result logs fit
+        // 1 GiB; spilled queries go to the exact kernel
         const int RE = lqg::replay_pool_regs(b.ef0);
         if (RE == 0) return fail(LQG_ERR_ARG, "ef too large for the replay kernel");
-        SearchArgs h = base_args(ix, w, b);
-        h.qhead = w.d_ctl + kCtlHeapHead;
-        h.vbits = t.visited_bits;
         lqg::ReplayArgs ra{};
         ra.rcap = (b.ef0 + 2u) & ~1u;
+        ra.efcap = std::min(32u * (uint32_t)RE - 32u, ra.rcap - 1u);
         ra.scap = t.heap_scap;
         ra.spill = w.d_spill;
         ra.nspill = w.d_ctl + kCtlSpilled;
+        ra.rlog_cap = std::max(1024u, 16u * b.ef0);
+        const int64_t chunk = std::min<int64_t>(
+            b.m, std::max<int64_t>(1024, (int64_t(1) << 30) / ((int64_t)ra.rlog_cap * 16)));
+        if ((s = grow(w.d_rlog, w.cap_rlog, (size_t)chunk * ra.rlog_cap)) != LQG_OK) return s;
+        if ((s = grow(w.d_rlen, w.cap_rlen, (size_t)chunk)) != LQG_OK) return s;
+        ra.rlog = w.d_rlog;
+        ra.rlen = w.d_rlen;
         int sw = plain ? 1 : (int)t.replay_warps;
-        while (sw > 1 && lqg::replay_smem_bytes(ix->dim, t.visited_bits, ra.rcap, ra.scap, sw) >
-                             227 * 1024)
+        while (sw > 1 && lqg::replay_smem_bytes(ix->dim, t.visited_bits, ra.scap, sw) > 227 * 1024)
             --sw;
         ra.swarps = (uint32_t)sw;
+        SearchArgs h = base_args(ix, w, b);
+        h.qhead = w.d_ctl + kCtlHeapHead;
+        h.vbits = t.visited_bits;
         int rb = 1;
         if (!plain) {
             int occ = 0;
@@ -227,7 +235,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             if (e != cudaSuccess || occ <= 0)
                 return fail(LQG_ERR_ARG, "replay kernel cannot launch with this tuning");
             rb = occ * ix->num_sms;
-            const int64_t need = (b.m + sw - 1) / sw;
+            const int64_t need = (chunk + sw - 1) / sw;
             if (need < rb) rb = (int)need;
         }
         const size_t slots = (size_t)rb * sw;
@@ -243,8 +251,38 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         ra.sp_global = w.d_sp_global;
         ra.gcap = kHeapGlobalCap;
         if (ix->ev_start) LQG_CUDA(cudaEventRecord(ix->ev_start, b.st));
-        e = lqg::launch_replay(h, ra, RE, (int)t.lanes_per_cand, degw, rb, b.st, nullptr);
-        if (e != cudaSuccess) return cuda_fail(e, "replay search launch");
+        for (int64_t off = 0; off < b.m; off += chunk) {
+            const int64_t mc = std::min(chunk, b.m - off);
+            if (off > 0) {  // fresh work-queue heads and spill list for this chunk
+                LQG_CUDA(cudaMemsetAsync(w.d_ctl + kCtlExactHead, 0, sizeof(uint32_t), b.st));
+                LQG_CUDA(cudaMemsetAsync(w.d_ctl + kCtlHeapHead, 0, 2 * sizeof(uint32_t), b.st));
+            }
+            SearchArgs c = h;
+            c.queries += off * ix->dim;
+            if (c.kq) c.kq += off;
+            if (c.efq) c.efq += off;
+            c.ids += off * b.kstride;
+            if (c.pool_ids) {
+                c.pool_ids += off * b.pstride;
+                c.pool_d += off * b.pstride;
+            }
+            if (c.stats) c.stats += off * 4;
+            c.m = mc;
+            const int cb = (int)std::min<int64_t>(rb, (mc + sw - 1) / sw);
+            e = lqg::launch_replay(c, ra, RE, (int)t.lanes_per_cand, degw, cb, b.st, nullptr);
+            if (e != cudaSuccess) return cuda_fail(e, "replay search launch");
+            e = lqg::launch_rp_replay(c, ra, b.st);
+            if (e != cudaSuccess) return cuda_fail(e, "result replay launch");
+            SearchArgs x = c;
+            x.qlist = w.d_spill;
+            x.nlist = w.d_ctl + kCtlSpilled;
+            x.qhead = w.d_ctl + kCtlExactHead;
+            e = lqg::launch_exact(x, w.xs, degw, plain ? 1 : w.x_warps_per_block,
+                                  plain ? 1 : w.x_blocks, b.st);
+            if (e != cudaSuccess) return cuda_fail(e, "exact search launch");
+        }
+        if (ix->ev_stop) LQG_CUDA(cudaEventRecord(ix->ev_stop, b.st));
+        return LQG_OK;
     } else {
 
     // 1. fast kernel over every query (mode 1); tied queries go to the list
@@ -662,11 +700,10 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         n.heap_scap = t->heap_scap;
     }
     if (t->replay_warps) {
-        if (t->replay_warps > 14) return fail(LQG_ERR_ARG, "replay_warps must be in [1, 14]");
+        if (t->replay_warps > 15) return fail(LQG_ERR_ARG, "replay_warps must be in [1, 15]");
         n.replay_warps = t->replay_warps;
     }
-    if (n.mode == 3 &&
-        lqg::replay_smem_bytes(ix->dim, n.visited_bits, kMaxEf + 2, n.heap_scap, 1) > 227 * 1024)
+    if (n.mode == 3 && lqg::replay_smem_bytes(ix->dim, n.visited_bits, n.heap_scap, 1) > 227 * 1024)
         return fail(LQG_ERR_ARG, "replay kernel tuning needs more than 227 KB of shared memory");
     if (n.mode != 3 &&
         lqg::heap_smem_bytes(ix->dim, n.visited_bits, kMaxEf + 2, n.heap_scap, (int)n.heap_warps) >

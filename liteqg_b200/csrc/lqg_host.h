@@ -57,6 +57,9 @@ struct Workspace {
     int64_t flagged_cap = 0;
     ExactScratch xs{};
     uint2* d_sp_global = nullptr;  // heap kernel: search-pool slots beyond shared memory
+    uint4* d_rlog = nullptr;       // replay kernel: per-query result logs
+    uint32_t* d_rlen = nullptr;    // replay kernel: per-query log lengths
+    size_t cap_rlog = 0, cap_rlen = 0;
     size_t sp_global_slots = 0;    // warps covered
     int x_blocks = 0, x_warps_per_block = 4;
     float* d_q = nullptr;
@@ -77,6 +80,9 @@ struct Workspace {
         dfree(xs.sp);
         dfree(xs.rp);
         dfree(d_sp_global);
+        dfree(d_rlog);
+        dfree(d_rlen);
+        cap_rlog = cap_rlen = 0;
         sp_global_slots = 0;
         dfree(d_q);
         dfree(d_kq);
@@ -160,7 +166,7 @@ struct lqg_index {
     lqg_host::Workspace ws;  // the default work area (one batch at a time)
 
     cudaStream_t own_stream = nullptr;
-    lqg_tuning tune{4, 10, 8, 0, 1, 4, 1024, 14};
+    lqg_tuning tune{4, 10, 8, 0, 1, 4, 1024, 15};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // recorded around the fast kernel
 
     ~lqg_index() {

@@ -43,30 +43,36 @@ size_t heap_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t rcap, uint32_t sca
 cudaError_t launch_heap(const SearchArgs& a, const HeapArgs& h, int G, int degw, int warps,
                         int blocks, cudaStream_t st, int* occ);
 
-// Replay kernel (replay_kernel.cuh): sorted-pool search warps plus two
-// heap-replay warps per block. E = replay_pool_regs(ef_max) (0: ef too large).
+// Replay kernel (replay_kernel.cuh): sorted-pool search warps plus one
+// search-heap replay warp per block, then a result-heap replay pass (one
+// thread per query). E = replay_pool_regs(ef_max) (0: ef too large).
 struct ReplayArgs {
-    uint32_t swarps;     // search warps per block (the replay warps follow)
-    uint32_t rcap;       // result-heap slots (>= ef + 1), shared memory
+    uint32_t swarps;     // search warps per block (the replay warp follows)
     uint32_t scap;       // search-heap slots in shared memory
     uint2* sp_global;    // [blocks * swarps][gcap] further search-heap slots
     uint32_t gcap;
     int32_t* spill;      // queries handed to the exact kernel
     uint32_t* nspill;
+    uint4* rlog;         // [m][rlog_cap] (id, distance, bound after, 0) per accepted node
+    uint32_t rlog_cap;
+    uint32_t* rlen;      // [m] accepted nodes logged, 0xFFFFFFFF if the search failed
+    uint32_t rcap;       // result-heap slots (>= ef + 1) of the replay pass
+    uint32_t efcap;      // largest ef: min(sorted-pool slots - 32, rcap - 1)
 };
-constexpr uint32_t kReplayLogN = 128;  // log ring entries (16 bytes) per search warp
+constexpr uint32_t kReplayLogN = 128;  // search-heap log ring entries (8 bytes) per search warp
 
 // Shared memory of one search warp: query, visited cache, candidates, log
-// ring, result heap, search heap, control words.
-__host__ __device__ inline size_t replay_warp_bytes(uint32_t dim, uint32_t vbits, uint32_t rcap,
-                                                    uint32_t scap) {
+// ring, search heap, control words.
+__host__ __device__ inline size_t replay_warp_bytes(uint32_t dim, uint32_t vbits, uint32_t scap) {
     const size_t dpad = (dim + 15u) & ~15u;
-    return 4 * dpad + 4 * ((size_t)1 << vbits) + kCandBytes + 16 * (size_t)kReplayLogN +
-           8 * (size_t)rcap + 8 * (size_t)scap + 16;
+    return 4 * dpad + 4 * ((size_t)1 << vbits) + kCandBytes + 8 * (size_t)kReplayLogN +
+           8 * (size_t)scap + 16;
 }
 int replay_pool_regs(uint32_t ef_max);
-size_t replay_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t rcap, uint32_t scap, int swarps);
+size_t replay_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t scap, int swarps);
 cudaError_t launch_replay(const SearchArgs& a, const ReplayArgs& ra, int E, int G, int degw,
                           int blocks, cudaStream_t st, int* occ);
+// Result-heap replay pass over a[0, m): one thread per query.
+cudaError_t launch_rp_replay(const SearchArgs& a, const ReplayArgs& ra, cudaStream_t st);
 
 }  // namespace lqg

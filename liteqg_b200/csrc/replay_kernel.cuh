@@ -1,12 +1,11 @@
-// Replay search kernel: the reference's search loop (QuantizedGraph::
+// Replay search: the reference's search loop (QuantizedGraph::
 // search_qg_with_heap, symqglib/qg/qg.hpp:298-344), exact for every query,
 // ties included, with the libstdc++ heap work taken off the search's critical
-// path.
+// path. Two kernels:
 //
-// A block holds S search warps (one query each, persistent over the work
-// queue) and two replay warps: lane j of the first runs the reference's result
-// pool (a std::priority_queue) for search warp j, lane j of the second its
-// search pool.
+// replay_search_kernel: a block holds S search warps (one query each,
+// persistent over the work queue) and one replay warp whose lane j runs the
+// reference's search pool (a std::priority_queue) for search warp j.
 //
 // Search warp. It needs only three things from the pools, and none of them
 // depends on how equal distances sit in the heaps:
@@ -22,24 +21,28 @@
 //     (E entries per lane, "popped" flag in bit 31 of the id). The smallest
 //     unpopped entry is sp.top() unless another unpopped entry has the same
 //     distance; only then does the heap layout decide, and the warp asks the
-//     search-heap replay lane for sp.top().
+//     replay lane for sp.top().
 // Neighbours are accepted in list order against the current size and bound
-// (qg.hpp:329-335). Every pool operation goes to a per-warp log ring in
-// shared memory: PUSH(id, dist, bound after), POP(id, bound), BEGIN(query),
-// END(bound).
+// (qg.hpp:329-335). The search-pool operations go to a per-warp log ring in
+// shared memory (PUSH(id, dist), POP(id), BEGIN(query), END(bound)); every
+// accepted node also goes to the query's result log in global memory
+// (id, dist, bound after).
 //
-// Replay lanes. Two lanes per search warp (one in each replay warp) replay its
-// log, one on the result heap and one on the search heap, laid out exactly as
-// GCC libstdc++'s push_heap/pop_heap leave them (bits/stl_heap.h: push =
-// sift-up while comp(parent, value); pop = hole from the root to a leaf along
-// the larger child, the right one unless comp(right, left), then sift-up of
-// the last element). They check the search warp at every step (each PUSH
-// passes the reference's acceptance test on the real result heap and leaves
-// rp.top() at the logged bound; each POP is sp.top(); at END the reference's
-// loop would stop), the search-heap lane answers tie questions, and the
-// result-heap lane writes the output by popping rp (qg.hpp:340-343). A query
-// that fails a check, or outgrows a pool, goes to the exact global-memory
-// kernel through the spill list.
+// Replay lane. It replays the ring on a search heap laid out exactly as GCC
+// libstdc++'s push_heap/pop_heap leave it (bits/stl_heap.h: push = sift-up
+// while comp(parent, value); pop = hole from the root to a leaf along the
+// larger child, the right one unless comp(right, left), then sift-up of the
+// last element), checks that each POP is sp.top() and that at END the
+// reference's loop would stop, and answers the tie questions.
+//
+// rp_replay_kernel (one thread per query, after the search): replays the
+// result log on a result heap laid out as libstdc++ leaves it, checks each
+// accepted node against the reference's acceptance test on that heap and the
+// logged bound against rp.top(), and writes the output by popping rp
+// (qg.hpp:340-343).
+//
+// A query that fails a check, or outgrows a pool or its log, goes to the exact
+// global-memory kernel through the spill list.
 //
 // Visited set: a direct-mapped cache of evaluated ids in shared memory. It may
 // forget an id, never invents one. A forgotten node that is evaluated again
@@ -77,10 +80,9 @@ constexpr uint32_t kOpFinish = 0xFFFFFFF4u;
 constexpr uint32_t kSpinLimit = 1u << 24;
 
 struct Ctl {
-    uint32_t head;     // log entries written (search warp)
-    uint32_t tail_rp;  // log entries replayed on the result heap
-    uint32_t tail_sp;  // log entries replayed on the search heap
-    uint32_t pad;
+    uint32_t head;  // ring entries written (search warp)
+    uint32_t tail;  // ring entries replayed (replay lane)
+    uint32_t pad0, pad1;
 };
 
 __device__ __forceinline__ uint32_t load_acq(uint32_t* p) {
@@ -346,7 +348,7 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
     float* pscale = pmin + dpad;
     const uint32_t vbits = a.vbits;
     const uint32_t vsize = 1u << vbits;
-    const size_t wbytes = replay_warp_bytes(dim, vbits, ra.rcap, ra.scap);
+    const size_t wbytes = replay_warp_bytes(dim, vbits, ra.scap);
     unsigned char* const base0 = smem + 8u * dpad;
 
     for (uint32_t i = threadIdx.x; i < dpad; i += blockDim.x) {
@@ -356,158 +358,89 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
     if ((uint32_t)warp < S && lane == 0) {
         Ctl* c = reinterpret_cast<Ctl*>(base0 + (size_t)warp * wbytes + wbytes - sizeof(Ctl));
         c->head = 0;
-        c->tail_rp = 0;
-        c->tail_sp = 0;
+        c->tail = 0;
     }
     __shared__ uint32_t block_abort;
     if (threadIdx.x == 0) block_abort = 0;
     __syncthreads();
 
-    // per-warp region: query | visited cache | candidates | log | rp | sp | ctl
+    // per-warp region: query | visited cache | candidates | ring | sp | ctl
     auto region = [&](uint32_t j) { return base0 + (size_t)j * wbytes; };
     auto ring_of = [&](unsigned char* wb) {
-        return reinterpret_cast<uint4*>(wb + 4u * dpad + 4u * vsize + kCandBytes);
+        return reinterpret_cast<uint2*>(wb + 4u * dpad + 4u * vsize + kCandBytes);
     };
-    auto rp_of = [&](unsigned char* wb) {
-        return reinterpret_cast<uint2*>(wb + 4u * dpad + 4u * vsize + kCandBytes + 16u * kLogN);
+    auto sp_of = [&](unsigned char* wb) {
+        return reinterpret_cast<uint2*>(wb + 4u * dpad + 4u * vsize + kCandBytes + 8u * kLogN);
     };
 
-    if ((uint32_t)warp >= S) {
-        // ====== replay warps: warp S runs the result heaps, warp S+1 the search
-        // heaps; lane j replays search warp j's log ======
-        const bool is_rp = (uint32_t)warp == S;
+    if ((uint32_t)warp == S) {
+        // ====== replay warp: lane j runs search warp j's search heap ======
         const uint32_t j = (uint32_t)lane;
         bool fin = j >= S;
         unsigned char* wb = region(fin ? 0u : j);
-        const uint4* ring = ring_of(wb);
+        const uint2* ring = ring_of(wb);
         Ctl* ctl = reinterpret_cast<Ctl*>(wb + wbytes - sizeof(Ctl));
-        uint32_t* my_tail = is_rp ? &ctl->tail_rp : &ctl->tail_sp;
-        const uint32_t rp_s = (uint32_t)__cvta_generic_to_shared(rp_of(wb));
-        const Heap rp{rp_s, nullptr, ra.rcap};
         const size_t gw = (size_t)blockIdx.x * S + j;
-        const Heap sp{rp_s + 8u * ra.rcap, ra.sp_global + (fin ? 0 : gw) * ra.gcap, ra.scap};
+        const Heap sp{(uint32_t)__cvta_generic_to_shared(sp_of(wb)),
+                      ra.sp_global + (fin ? 0 : gw) * ra.gcap, ra.scap};
         const uint32_t sp_max = ra.scap + ra.gcap;
         uint32_t tail = 0, released = 0, head_c = 0;
         int64_t qi = 0;
-        uint32_t ef = 1, k = 1, n = 0, P = 0, ex_j = 0, ex_n = 0;
-        bool err = false, extracting = false;
+        uint32_t n = 0;
+        bool err = false;
         uint32_t idle = 0;
         auto spill = [&]() {
             const uint32_t i = atomicAdd(ra.nspill, 1u);
             ra.spill[i] = (int32_t)qi;
+            ra.rlen[qi] = kNoId;  // the result pass skips it
         };
         for (;;) {
-            bool progressed = false, dopop = false, check = false;
+            bool progressed = false, dopop = false;
             uint32_t pn = 0;
-            float want_lower = 0.f;
             if (!fin) {
-                if (extracting) {
-                    // qg.hpp:340-343: results[k-1-j] = j-th pop of rp
-                    const uint2 t = rp.get(0);
-                    if (ex_j < k && ex_j < P) a.ids[qi * a.kstride + (k - 1 - ex_j)] = t.x;
-                    if (a.pool_ids) {
-                        const uint32_t pos = P - 1 - ex_j;
-                        if (pos < a.pstride) {
-                            a.pool_ids[qi * a.pstride + pos] = t.x;
-                            a.pool_d[qi * a.pstride + pos] = hkey(t);
-                        }
-                    }
-                    dopop = true;
-                    pn = n;
-                    --n;
-                    if (++ex_j == ex_n) extracting = false;
+                if (tail == head_c) head_c = load_acq(&ctl->head);
+                if (tail != head_c) {
+                    const uint2 e = ring[tail % kLogN];
+                    ++tail;
                     progressed = true;
-                } else {
-                    if (tail == head_c) head_c = load_acq(&ctl->head);
-                    if (tail != head_c) {
-                        const uint4 e = ring[tail % kLogN];
-                        ++tail;
-                        progressed = true;
-                        if (e.y == kOpBegin) {
-                            qi = (int64_t)e.x;
-                            const uint32_t efq = a.efq ? a.efq[qi] : a.ef0;
-                            ef = min(min(max(efq, 1u), 32u * E - 32u), ra.rcap - 1u);
-                            k = min(a.kq ? a.kq[qi] : a.k0, a.kstride);
-                            n = 0;
-                            err = false;
-                        } else if (e.y == kOpFinish) {
-                            fin = true;
-                        } else if (is_rp) {
-                            if (e.y == kOpPop) {
-                                // the bound the search warp used for this pop's candidates
-                                if (!err && (n == 0 || hkey(rp.get(0)) != __uint_as_float(e.z)))
-                                    err = true;
-                            } else if (e.y == kOpEnd || e.y == kOpEndFail) {
-                                const bool ok = !err && e.y == kOpEnd && n > 0 &&
-                                                hkey(rp.get(0)) == __uint_as_float(e.z);
-                                if (!ok) {
-                                    spill();
-                                } else {
-                                    P = n;
-                                    const uint32_t kk = min(k, P);
-                                    for (uint32_t x = 0; x < k - kk; ++x)
-                                        a.ids[qi * a.kstride + x] = kNoId;
-                                    if (a.pool_ids)
-                                        for (uint32_t x = P; x < a.pstride; ++x) {
-                                            a.pool_ids[qi * a.pstride + x] = kNoId;
-                                            a.pool_d[qi * a.pstride + x] = CUDART_INF_F;
-                                        }
-                                    ex_j = 0;
-                                    ex_n = a.pool_ids ? P : kk;
-                                    extracting = ex_n > 0;
-                                }
-                            } else if (!err) {
-                                // PUSH (qg.hpp:329-335): the reference's test on the real heap
-                                const float y = __uint_as_float(e.y);
-                                if (!(n < ef || hkey(rp.get(0)) > y)) {
-                                    err = true;
-                                } else {
-                                    sift_up(rp, n, make_uint2(e.x, e.y));
-                                    ++n;
-                                    if (n > ef) {
-                                        dopop = true;
-                                        pn = n;
-                                        --n;
-                                    }
-                                    check = true;
-                                    want_lower = __uint_as_float(e.z);
-                                }
+                    if (e.y == kOpBegin) {
+                        qi = (int64_t)e.x;
+                        n = 0;
+                        err = false;
+                    } else if (e.y == kOpPop) {
+                        // qg.hpp:314-318: the search warp popped sp.top()
+                        if (!err) {
+                            if (n == 0 || sp.get(0).x != e.x) {
+                                err = true;
+                            } else {
+                                dopop = true;
+                                pn = n;
+                                --n;
                             }
+                        }
+                    } else if (e.y == kOpEnd) {
+                        // the reference's loop stops here: sp empty or its top above the bound
+                        const bool ok = !err && (n == 0 || -hkey(sp.get(0)) > __uint_as_float(e.x));
+                        if (!ok) spill();
+                    } else if (e.y == kOpEndFail) {
+                        spill();
+                    } else if (e.y == kOpFinish) {
+                        fin = true;
+                    } else if (!err) {
+                        // PUSH (qg.hpp:330)
+                        if (n >= sp_max) {
+                            err = true;
                         } else {
-                            if (e.y == kOpPop) {
-                                // qg.hpp:314-318: the search warp popped sp.top()
-                                if (!err) {
-                                    if (n == 0 || sp.get(0).x != e.x) {
-                                        err = true;
-                                    } else {
-                                        dopop = true;
-                                        pn = n;
-                                        --n;
-                                    }
-                                }
-                            } else if (e.y == kOpEnd) {
-                                // the reference's loop stops here: sp empty or its top above the bound
-                                const bool ok =
-                                    !err && (n == 0 || -hkey(sp.get(0)) > __uint_as_float(e.z));
-                                if (!ok) spill();
-                            } else if (e.y != kOpEndFail && !err) {
-                                // PUSH
-                                if (n >= sp_max) {
-                                    err = true;
-                                } else {
-                                    sift_up(sp, n, make_uint2(e.x, __float_as_uint(-__uint_as_float(e.y))));
-                                    ++n;
-                                }
-                            }
+                            sift_up(sp, n, make_uint2(e.x, __float_as_uint(-__uint_as_float(e.y))));
+                            ++n;
                         }
                     }
                 }
             }
-            if (dopop) pop_top(is_rp ? rp : sp, pn);
-            if (check && hkey(rp.get(0)) != want_lower) err = true;
+            if (dopop) pop_top(sp, pn);
             // publish progress when caught up, or every 16 entries
             if (j < S && tail != released && (tail == head_c || tail - released >= 16 || fin)) {
-                store_rel(my_tail, tail);
+                store_rel(&ctl->tail, tail);
                 released = tail;
             }
             if (!__ballot_sync(kFull, !fin)) break;
@@ -532,8 +465,8 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
     uint32_t* vis = reinterpret_cast<uint32_t*>(wb + 4u * dpad);
     uint32_t* cid = vis + vsize;
     float* cd = reinterpret_cast<float*>(cid + kMaxDeg);
-    uint4* ring = ring_of(wb);
-    const uint2* sp_top = rp_of(wb) + ra.rcap;
+    uint2* ring = ring_of(wb);
+    const uint2* sp_top = sp_of(wb);
     Ctl* ctl = reinterpret_cast<Ctl*>(wb + wbytes - sizeof(Ctl));
 
     const int g = lane / G, r = lane % G;
@@ -544,20 +477,19 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
     constexpr int NP = G;  // passes per distance batch: 32 candidates
     constexpr uint32_t BATCH = (uint32_t)NP * (32 / G);
 
-    // log writer state (lane 0)
+    // ring writer state (lane 0)
     uint32_t head = 0, tail_c = 0;
     bool aborted = false;
     auto publish = [&]() {
         if (lane == 0) store_rel(&ctl->head, head);
     };
-    // lane 0 appends one entry; waits (bounded) for room
-    auto put = [&](uint4 e) {
+    // lane 0 appends one ring entry; waits (bounded) for room
+    auto put = [&](uint2 e) {
         if (lane == 0 && !aborted) {
             if (head - tail_c >= kLogN) {
                 store_rel(&ctl->head, head);
                 uint32_t spin = 0;
-                while (head - (tail_c = min(load_acq(&ctl->tail_rp), load_acq(&ctl->tail_sp))) >=
-                       kLogN) {
+                while (head - (tail_c = load_acq(&ctl->tail)) >= kLogN) {
                     if (++spin > kSpinLimit || load_rlx(&block_abort)) {
                         atomicOr(a.err, kErrSync);
                         atomicExch(&block_abort, 1u);
@@ -581,11 +513,12 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
         if ((int64_t)slot >= mlist || slot == 0xFFFFFFFFu) break;
         const int64_t qi = a.qlist ? (int64_t)a.qlist[slot] : (int64_t)slot;
         uint32_t ef = a.efq ? a.efq[qi] : a.ef0;
-        ef = min(min(max(ef, 1u), CAP - 32u), ra.rcap - 1u);
+        ef = min(max(ef, 1u), ra.efcap);  // efcap <= CAP - 32
         const float* q = a.queries + (size_t)qi * dim;
+        uint4* rlog = ra.rlog + (size_t)qi * ra.rlog_cap;
         for (uint32_t i = lane; i < dpad; i += 32) qs[i] = i < dim ? q[i] : 0.f;
         for (uint32_t i = lane; i < vsize; i += 32) vis[i] = kNoId;
-        put(make_uint4((uint32_t)qi, kOpBegin, 0u, 0u));
+        put(make_uint2((uint32_t)qi, kOpBegin));
         __syncwarp();
 
         float pd[E];
@@ -609,8 +542,9 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
             pd[0] = d0;
             pi[0] = ep;
             vis[hash_id(ep, vbits)] = ep;
+            rlog[0] = make_uint4(ep, __float_as_uint(d0), __float_as_uint(d0), 0u);
         }
-        put(make_uint4(ep, __float_as_uint(d0), __float_as_uint(d0), 0u));
+        put(make_uint2(ep, __float_as_uint(d0)));
         __syncwarp();
         uint32_t pops = 0, calcs = 1;
 
@@ -645,12 +579,12 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
                 }
                 u = __shfl_sync(kFull, mu, owner);
             } else {
-                // equal distances: the heap layout decides; ask the search-heap lane
+                // equal distances: the heap layout decides; ask the replay lane
                 uint32_t top = kNoId;
                 if (lane == 0 && !aborted) {
                     store_rel(&ctl->head, head);
                     uint32_t spin = 0;
-                    while (load_acq(&ctl->tail_sp) != head) {
+                    while (load_acq(&ctl->tail) != head) {
                         if (++spin > kSpinLimit || load_rlx(&block_abort)) {
                             atomicOr(a.err, kErrSync);
                             atomicExch(&block_abort, 1u);
@@ -659,6 +593,7 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
                         }
                         __nanosleep(32);
                     }
+                    tail_c = head;
                     if (!aborted) top = sp_top[0].x;
                 }
                 u = __shfl_sync(kFull, top, 0);
@@ -674,7 +609,7 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
                     break;
                 }
             }
-            put(make_uint4(u, kOpPop, __float_as_uint(lower), 0u));
+            put(make_uint2(u, kOpPop));
             ++pops;
 
             // ---- qg.hpp:320-324: unvisited neighbours in list order ----
@@ -730,8 +665,8 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
 #pragma unroll
                     for (int t = 0; t < E; ++t) dup |= pd[t] == y && (pi[t] & ~kExpanded) == id;
                     if (__any_sync(kFull, dup)) continue;
-                    // room for one more entry (ties at the bound can exceed ef)
-                    if (__shfl_sync(kFull, pd[E - 1], 31) < INF) {
+                    // room for one more entry (ties at the bound can exceed ef), and in the log
+                    if (__shfl_sync(kFull, pd[E - 1], 31) < INF || acc_n >= ra.rlog_cap) {
                         fail = true;
                         break;
                     }
@@ -755,9 +690,8 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
                             pi[t] = ni;
                         }
                     }
-                    ++acc_n;
-                    lower = rpool_at<E>(pd, min(acc_n, ef) - 1);
-                    if (acc_n > ef) {
+                    lower = rpool_at<E>(pd, min(acc_n + 1, ef) - 1);
+                    if (acc_n + 1 > ef) {
                         // beyond the ef-th entry only ties with the bound stay poppable
 #pragma unroll
                         for (int t = 0; t < E; ++t) {
@@ -768,7 +702,10 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
                             }
                         }
                     }
-                    put(make_uint4(id, __float_as_uint(y), __float_as_uint(lower), 0u));
+                    if (lane == 0)
+                        rlog[acc_n] = make_uint4(id, __float_as_uint(y), __float_as_uint(lower), 0u);
+                    ++acc_n;
+                    put(make_uint2(id, __float_as_uint(y)));
                 }
                 if (fail) break;
             }
@@ -776,7 +713,8 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
             if (__shfl_sync(kFull, (int)aborted, 0)) fail = true;
         }
 
-        put(make_uint4(0u, fail ? kOpEndFail : kOpEnd, __float_as_uint(lower), 0u));
+        if (lane == 0) ra.rlen[qi] = fail ? kNoId : acc_n;
+        put(make_uint2(fail ? 0u : __float_as_uint(lower), fail ? kOpEndFail : kOpEnd));
         publish();
         if (a.stats && lane == 0) {
             const uint32_t P = min(acc_n, ef);
@@ -785,7 +723,7 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
         __syncwarp();
         if (__shfl_sync(kFull, (int)aborted, 0)) break;
     }
-    put(make_uint4(0u, kOpFinish, 0u, 0u));
+    put(make_uint2(0u, kOpFinish));
     publish();
 }
 
@@ -794,11 +732,11 @@ static cudaError_t replay_run(const SearchArgs& a, const ReplayArgs& ra, int blo
                              cudaStream_t st, int* occ) {
     const size_t dpad = (a.dim + 15u) & ~15u;
     const size_t smem =
-        8 * dpad + (size_t)ra.swarps * replay_warp_bytes(a.dim, a.vbits, ra.rcap, ra.scap);
+        8 * dpad + (size_t)ra.swarps * replay_warp_bytes(a.dim, a.vbits, ra.scap);
     auto k = replay_search_kernel<E, G, DEGW>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int threads = 32 * ((int)ra.swarps + 2);
+    const int threads = 32 * ((int)ra.swarps + 1);
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, threads, smem);
     k<<<blocks, threads, smem, st>>>(a, ra);
     return cudaGetLastError();

@@ -68,7 +68,7 @@ def test_replay_pools_and_pops_bit_exact(lqg, golden):
 
 
 @pytest.mark.parametrize("g_lanes,vbits,swarps,scap", [
-    (4, 10, 14, 512), (2, 8, 4, 256), (8, 13, 1, 2048), (4, 9, 7, 1024), (2, 12, 14, 256)])
+    (4, 10, 15, 512), (2, 8, 4, 256), (8, 13, 1, 2048), (4, 9, 7, 1024), (2, 12, 15, 256)])
 def test_replay_tuning_does_not_change_results(lqg, golden, g_lanes, vbits, swarps, scap):
     for name in ("mix128d64", "bin40"):
         g = golden[name]
