@@ -29,6 +29,7 @@
 
 #include "lqg_internal.h"
 #include "lqg_kernels.cuh"
+#include "sq8_batch.cuh"
 
 namespace lqg {
 
@@ -118,7 +119,7 @@ __device__ __forceinline__ void warp_pop(HeapView h, uint32_t& n, int lane) {
 }  // namespace
 
 template <int G, int DEGW>
-__global__ void __launch_bounds__(256, 1) heap_search_kernel(SearchArgs a, HeapArgs hp) {
+__global__ void __launch_bounds__(256, 2) heap_search_kernel(SearchArgs a, HeapArgs hp) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -146,7 +147,6 @@ __global__ void __launch_bounds__(256, 1) heap_search_kernel(SearchArgs a, HeapA
     __syncthreads();
 
     const int g = lane / G, r = lane % G;
-    constexpr int CPP = 32 / G;
     const uint32_t lt = lanemask_lt();
     const int64_t mlist = a.nlist ? (int64_t)*a.nlist : a.m;
 
@@ -166,9 +166,11 @@ __global__ void __launch_bounds__(256, 1) heap_search_kernel(SearchArgs a, HeapA
 
         // qg.hpp:305-311
         const uint32_t ep = a.entry;
-        float d0 = sq8_l2_group<G>(a.codes + (size_t)ep * a.cstride, g == 0, qs, pmin, pscale,
-                                   dim, r);
-        d0 = __shfl_sync(kFull, d0, 0);
+        if (lane == 0) cid[0] = ep;
+        __syncwarp();
+        eval_batch<G, G>(a, cid, cd, 0, 1, qs, pmin, pscale, g, r);
+        __syncwarp();
+        const float d0 = cd[0];
         uint32_t sn = 0, rn = 0;
         if (lane == 0) {
             sp.set(0, make_uint2(ep, __float_as_uint(-d0)));
@@ -212,14 +214,8 @@ __global__ void __launch_bounds__(256, 1) heap_search_kernel(SearchArgs a, HeapA
             }
 
             // qg.hpp:325-328
-            for (uint32_t base = 0; base < ncand; base += CPP) {
-                const uint32_t c = base + g;
-                const bool valid = c < ncand;
-                const uint32_t id = valid ? cid[c] : 0u;
-                const float d = sq8_l2_group<G>(a.codes + (size_t)id * a.cstride, valid, qs, pmin,
-                                                pscale, dim, r);
-                if (valid && r == 0) cd[c] = d;
-            }
+            for (uint32_t b = 0; b < ncand; b += 32)
+                eval_batch<G, G>(a, cid, cd, b, ncand, qs, pmin, pscale, g, r);
             calcs += ncand;
             __syncwarp();
 

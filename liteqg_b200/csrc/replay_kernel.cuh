@@ -62,6 +62,7 @@
 
 #include "lqg_internal.h"
 #include "lqg_kernels.cuh"
+#include "sq8_batch.cuh"
 
 namespace lqg {
 
@@ -165,162 +166,6 @@ __device__ __forceinline__ void pop_top(const Heap& h, uint32_t n) {
         hole = second - 1;
     }
     sift_up(h, hole, v);
-}
-
-// ---- packed FP32 pairs -----------------------------------------------------
-
-__device__ __forceinline__ unsigned long long pk(uint32_t lo, uint32_t hi) {
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(lo), "r"(hi));
-    return r;
-}
-__device__ __forceinline__ void upk(unsigned long long v, float& lo, float& hi) {
-    uint32_t a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=r"(a), "=r"(b) : "l"(v));
-    lo = __uint_as_float(a);
-    hi = __uint_as_float(b);
-}
-__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
-                                                   unsigned long long c) {
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
-    unsigned long long d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-
-// Distances of candidates cid[base + p * (32/G) + g], p < NP, into cd[].
-// Lane r of group g owns accumulators [r*A, r*A + A) (A = 16/G); all code
-// bytes of a round of U chunks, for all NP passes, are requested before any
-// arithmetic. Passes with no valid candidate are skipped (warp-uniform).
-template <int G, int NP>
-__device__ __forceinline__ void eval_batch(const SearchArgs& a, const uint32_t* cid, float* cd,
-                                           uint32_t base, uint32_t ncand,
-                                           const float* __restrict__ qs,
-                                           const float* __restrict__ pmin,
-                                           const float* __restrict__ pscale, int g, int r) {
-    constexpr int A = 16 / G;
-    constexpr int W = (A + 3) / 4;
-    constexpr int CPP = 32 / G;
-    constexpr int UU = 32 / (NP * W);
-    constexpr int U = UU < 1 ? 1 : (UU > 8 ? 8 : UU);
-    constexpr int AP = A >= 2 ? A / 2 : 1;  // accumulator pairs
-    const uint32_t dim = a.dim;
-    const uint32_t mul = dim & ~15u;
-    const unsigned long long C23 = pk(0x4B000000u, 0x4B000000u);
-
-    const uint8_t* rowp[NP];
-    bool valid[NP];
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        const uint32_t c = base + p * CPP + g;
-        valid[p] = c < ncand;
-        rowp[p] = a.codes + (size_t)(valid[p] ? cid[c] : 0u) * a.cstride + r * A;
-    }
-    unsigned long long acc2[NP][AP];
-    float acc1[NP];
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        acc1[p] = 0.f;
-#pragma unroll
-        for (int t = 0; t < AP; ++t) acc2[p][t] = 0ull;
-    }
-    for (uint32_t b0 = 0; b0 < mul; b0 += 16 * U) {
-        uint32_t w[NP][U][W];
-#pragma unroll
-        for (int p = 0; p < NP; ++p)
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t b = b0 + 16 * u;
-                if (valid[p] && b < mul) {
-                    load_chunk<A>(rowp[p] + b, w[p][u]);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < W; ++i) w[p][u][i] = 0;
-                }
-            }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t b = b0 + 16 * u;
-            if (b >= mul) break;
-            const uint32_t d0 = b + r * A;
-            if constexpr (A >= 2) {
-                unsigned long long q2[AP], m2[AP], s2[AP];
-#pragma unroll
-                for (int t = 0; t < AP; ++t) {
-                    q2[t] = *reinterpret_cast<const unsigned long long*>(qs + d0 + 2 * t);
-                    m2[t] = *reinterpret_cast<const unsigned long long*>(pmin + d0 + 2 * t);
-                    s2[t] = *reinterpret_cast<const unsigned long long*>(pscale + d0 + 2 * t);
-                }
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    if (base + p * CPP >= ncand) continue;
-#pragma unroll
-                    for (int t = 0; t < AP; ++t) {
-                        const uint32_t wd = w[p][u][(2 * t) / 4];
-                        const int s0 = (2 * t) % 4;
-                        const uint32_t lo = __byte_perm(wd, 0x4B000000u, 0x7440u + s0);
-                        const uint32_t hi = __byte_perm(wd, 0x4B000000u, 0x7440u + s0 + 1);
-                        const unsigned long long c2 = sub2(pk(lo, hi), C23);
-                        const unsigned long long dec = fma2(c2, s2[t], m2[t]);
-                        const unsigned long long df = sub2(q2[t], dec);
-                        acc2[p][t] = fma2(df, df, acc2[p][t]);
-                    }
-                }
-            } else {
-                const float qv = qs[d0], mv = pmin[d0], sv = pscale[d0];
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    if (base + p * CPP >= ncand) continue;
-                    const float c = byte_to_float(w[p][u][0], 0);
-                    const float dec = __fmaf_rn(c, sv, mv);
-                    const float df = __fsub_rn(qv, dec);
-                    acc1[p] = __fmaf_rn(df, df, acc1[p]);
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        if (base + p * CPP >= ncand) break;  // warp-uniform
-        float acc[A];
-        if constexpr (A >= 2) {
-#pragma unroll
-            for (int t = 0; t < AP; ++t) upk(acc2[p][t], acc[2 * t], acc[2 * t + 1]);
-        } else {
-            acc[0] = acc1[p];
-        }
-        // the AVX-512 reduction tree (l2.hpp:16-35): fold 8, 4, 2, 1
-#pragma unroll
-        for (int h = 8; h >= 1; h >>= 1) {
-            if (h >= A) {
-#pragma unroll
-                for (int t = 0; t < A; ++t) {
-                    const float o = __shfl_down_sync(kFull, acc[t], h / A);
-                    acc[t] = __fadd_rn(acc[t], o);
-                }
-            } else {
-#pragma unroll
-                for (int t = 0; t < A; ++t)
-                    if (t < h) acc[t] = __fadd_rn(acc[t], acc[t + h]);
-            }
-        }
-        float res = acc[0];
-        const uint32_t c = base + p * CPP + g;
-        if (r == 0 && valid[p]) {
-            const uint8_t* row = a.codes + (size_t)cid[c] * a.cstride;
-            for (uint32_t d = mul; d < dim; ++d) {
-                const float cv = (float)row[d];
-                const float dec = __fmaf_rn(cv, pscale[d], pmin[d]);
-                const float df = __fsub_rn(qs[d], dec);
-                res = __fmaf_rn(df, df, res);
-            }
-            cd[c] = res;
-        }
-    }
 }
 
 }  // namespace replay
