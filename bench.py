@@ -48,14 +48,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "QPS @ recall@10≥0.95: batched vs plain GPU vs CPU; p50/p99 ms; HBM GB/s"
-BUILDER_VERSION = "gpu-builder-2"
+BUILDER_VERSION = "gpu-builder-3"
 
 WORKLOADS = {
     "batched-1m128": dict(n=1_000_000, dim=128, gen="int_mixture", clusters=1024, lo=0.0,
-                          hi=255.0, sigma=20.0, deg=32, efb=400, iters=3, random_edges=16,
-                          nq=10_000, k=10, efs=(64, 128, 256), k_extra=100),
+                          hi=255.0, sigma=20.0, deg=32, efb=400, iters=3, random_edges=8,
+                          path_take=64, far_budget=8, nq=10_000, k=10, efs=(64, 128, 256),
+                          k_extra=100),
     "small-100k64": dict(n=100_000, dim=64, gen="uniform", deg=32, efb=200, iters=3,
-                         random_edges=4, nq=1000, k=10, efs=(20, 40, 60, 100, 200), k_extra=100),
+                         random_edges=4, path_take=64, far_budget=4, nq=1000, k=10,
+                         efs=(20, 40, 60, 100, 200), k_extra=100),
 }
 
 
@@ -102,7 +104,8 @@ def get_index_file(name, w, base, device):
         return path, 0.0
     ix = liteqg_b200.Index("QG", "L2", w["n"], w["dim"], w["deg"], device=device)
     t = time.perf_counter()
-    ix.build_index(base, w["efb"], num_iter=w["iters"], random_edges=w["random_edges"])
+    ix.build_index(base, w["efb"], num_iter=w["iters"], random_edges=w["random_edges"],
+                   path_take=w["path_take"], far_budget=w["far_budget"])
     tb = time.perf_counter() - t
     tmp = path + f".tmp{os.getpid()}"
     ix.save(tmp)
@@ -478,7 +481,8 @@ def gpu_arm(args, w, name, rank, world, device):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']} "
-                               f"(random_edges={w['random_edges']}), {nq} queries/GPU, "
+                               f"(random_edges={w['random_edges']}, path_take={w['path_take']}, "
+                               f"far_budget={w['far_budget']}), {nq} queries/GPU, "
                                f"k={k}, ef={chosen}", "ef": chosen, "k": k,
                    "recall_at_10_pool": recall.get(chosen), "recall_by_ef": recall,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",

@@ -93,6 +93,23 @@ LQG_API lqg_status lqg_get_arrays(const lqg_index* ix, uint32_t* entry, float* v
 LQG_API lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build,
                              uint32_t num_iter, uint64_t seed, uint32_t random_edges);
 
+/* lqg_build with search-path long links (no reference counterpart; the
+ * reference's heuristic_prune, qg_builder.hpp:155-200, is alpha = 1,
+ * path_take = far_budget = 0, which lqg_build uses):
+ *   alpha >= 1   a kept neighbour j removes a later candidate i only when
+ *                alpha * |j - i| < |node - i|; alpha > 1 keeps longer, more
+ *                diverse links (the Vamana rule);
+ *   path_take    the first path_take nodes popped by each node's build search
+ *                (from the entry point toward the node) join its candidates,
+ *                up to 32 of them beyond the nearest ones;
+ *   far_budget   slots of each list that only candidates farther than twice
+ *                the nearest candidate's distance may take.
+ * With reverse edges these become routes from the entry region into every
+ * cluster of clustered data. */
+LQG_API lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build,
+                                uint32_t num_iter, uint64_t seed, uint32_t random_edges,
+                                float alpha, uint32_t path_take, uint32_t far_budget);
+
 /* Index.set_ef: symqglib/qg/qg.hpp:226-230. ef in [1, 512]. */
 LQG_API lqg_status lqg_set_ef(lqg_index* ix, uint32_t ef);
 

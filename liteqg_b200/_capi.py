@@ -32,6 +32,8 @@ SIGNATURES = {
     "lqg_get_arrays": (C.c_int, [_vp, _u32p, _vp, _vp, _vp, _vp]),
     "lqg_set_ef": (C.c_int, [_vp, C.c_uint32]),
     "lqg_build": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32]),
+    "lqg_build_ex": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
+                               C.c_float, C.c_uint32, C.c_uint32]),
     "lqg_search": (C.c_int, [_vp, _vp, C.c_uint32, _vp]),
     "lqg_search_batch_device": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
                                           _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),

@@ -13,7 +13,9 @@
 //
 // Pruning follows heuristic_prune (qg_builder.hpp:155-200): candidates in
 // ascending exact distance; a candidate is kept unless an already-kept one
-// lies closer to it than the node does (d(kept, c) < d(node, c)).
+// lies closer to it than the node does (d(kept, c) < d(node, c)); with an
+// occlusion factor alpha > 1 (squared distances: alpha^2 d(kept, c) <
+// d(node, c)) the longer links of the Vamana rule survive too.
 // The candidate-to-candidate distances of one node form a P x P matrix that
 // one CTA accumulates in registers over 128-dimension tiles staged in shared
 // memory.
@@ -225,24 +227,29 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     }
     __syncthreads();
 
-    // 1. gather (duplicates removed below after sorting by (id))
-    auto add = [&](uint32_t v) {
+    // 1. gather (duplicates removed below after sorting by id). Entries are
+    // id << 1 | from_path (ids < 2^31).
+    auto add = [&](uint32_t v, uint32_t from_path) {
         if (v == (uint32_t)node || v >= a.n) return;
         const uint32_t s = atomicAdd(&s_cnt, 1u);
-        if (s < kCandMax) s_ids[s] = v;
+        if (s < kCandMax) s_ids[s] = (v << 1) | from_path;
     };
     if (a.pool) {
         const uint32_t* p = a.pool + (node - a.node0) * a.pool_stride;
-        for (uint32_t j = tid; j < a.pool_take; j += kPruneThreads) add(p[j]);
+        for (uint32_t j = tid; j < a.pool_take; j += kPruneThreads) add(p[j], 0u);
+    }
+    if (a.path) {
+        const uint32_t* p = a.path + (node - a.node0) * a.path_stride;
+        for (uint32_t j = tid; j < a.path_take; j += kPruneThreads) add(p[j], 1u);
     }
     if (a.nb) {
         const uint32_t c = a.nb_cnt ? min(a.nb_cnt[node], a.deg) : a.deg;
-        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.nb[node * a.deg + j]);
+        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.nb[node * a.deg + j], 0u);
     }
     if (a.rev) {
         const uint32_t s0 = a.rev_start[node], s1 = a.rev_end[node];
         const uint32_t c = min(s1 - s0, a.rev_cap);
-        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.rev[s0 + j]);
+        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.rev[s0 + j], 0u);
     }
     __syncthreads();
     const uint32_t cnt = min(s_cnt, (uint32_t)kCandMax);
@@ -268,8 +275,10 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     const float* xn = a.x + node * dim;
     for (uint32_t i = tid; i < cnt; i += kPruneThreads) {
         const uint32_t v = s_ids[i];
-        const bool dup = i > 0 && s_ids[i - 1] == v;
-        s_d[i] = (dup || v == 0xFFFFFFFFu) ? CUDART_INF_F : l2_ref_order(xn, a.x + (uint64_t)v * dim, dim);
+        // keep the last of equal ids (the path-flagged copy, if any)
+        const bool dup = i + 1 < cnt && (s_ids[i + 1] >> 1) == (v >> 1);
+        s_d[i] = (dup || v == 0xFFFFFFFFu) ? CUDART_INF_F
+                                            : l2_ref_order(xn, a.x + (uint64_t)(v >> 1) * dim, dim);
     }
     __syncthreads();
     // 3. sort ascending by (distance, id)
@@ -302,7 +311,27 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         for (uint32_t i = tid; i < kCandMax; i += kPruneThreads)
             if (s_d[i] < CUDART_INF_F) atomicAdd(&s_valid, 1u);
         __syncthreads();
-        P = min(s_valid, (uint32_t)kPruneMax);
+        const uint32_t V = s_valid;
+        if (a.path && a.far_take && V > (uint32_t)kPruneMax) {
+            // the nearest kPruneMax - far_take, then search-path candidates
+            // beyond them in distance order; compacted in place
+            if (tid == 0) {
+                const uint32_t near = kPruneMax - min(a.far_take, (uint32_t)kPruneMax);
+                uint32_t w = near, taken = 0;
+                for (uint32_t i = near; i < V && taken < a.far_take; ++i)
+                    if (s_ids[i] & 1u) {
+                        s_ids[w] = s_ids[i];
+                        s_d[w] = s_d[i];
+                        ++w;
+                        ++taken;
+                    }
+                s_valid = w;
+            }
+            __syncthreads();
+            P = s_valid;
+        } else {
+            P = min(V, (uint32_t)kPruneMax);
+        }
     }
 
     // 4. pairwise distances among the first P candidates, tiled over dims.
@@ -335,7 +364,7 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         __syncthreads();
         for (uint32_t e = tid; e < P * td; e += kPruneThreads) {
             const uint32_t r = e / td, c = e % td;
-            tile[r * (kTileD + 1) + c] = a.x[(uint64_t)s_ids[r] * dim + d0 + c];
+            tile[r * (kTileD + 1) + c] = a.x[(uint64_t)(s_ids[r] >> 1) * dim + d0 + c];
         }
         __syncthreads();
 #pragma unroll
@@ -371,14 +400,21 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     // thread counts kept candidates in a register, so all threads take the
     // same branches.
     const uint32_t cap = a.out_cap ? min(a.out_cap, a.deg) : a.deg;
-    uint32_t kept_n = 0;
+    // far_budget slots are held for long links: a candidate farther than 4x
+    // the nearest one's squared distance; near ones stop at cap - far_budget
+    const uint32_t near_cap = a.far_budget < cap ? cap - a.far_budget : cap;
+    const float far_d = 4.0f * s_d[0];
+    uint32_t kept_n = 0, kept_near = 0;
     for (uint32_t j = 0; j < P; ++j) {
         if (s_state[j] != 0) continue;
         if (kept_n >= cap) break;
+        const bool is_far = a.far_budget != 0 && s_d[j] > far_d;
+        if (!is_far && kept_near >= near_cap) continue;
         ++kept_n;
+        if (!is_far) ++kept_near;
         if (tid == 0) s_keep[j] = 1;
         for (uint32_t i = j + 1 + tid; i < P; i += kPruneThreads)
-            if (s_state[i] == 0 && pair[j * kPruneMax + i] < s_d[i]) s_state[i] = 2;
+            if (s_state[i] == 0 && a.alpha2 * pair[j * kPruneMax + i] < s_d[i]) s_state[i] = 2;
         __syncthreads();
     }
     __syncthreads();
@@ -386,11 +422,11 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         uint32_t* out = a.out + node * a.deg;
         uint32_t w = 0;
         for (uint32_t j = 0; j < P && w < cap; ++j)
-            if (s_keep[j]) out[w++] = s_ids[j];
+            if (s_keep[j]) out[w++] = s_ids[j] >> 1;
         const uint32_t kept = w;
         if (a.fill)
             for (uint32_t j = 0; j < P && w < cap; ++j)
-                if (!s_keep[j]) out[w++] = s_ids[j];
+                if (!s_keep[j]) out[w++] = s_ids[j] >> 1;
         if (a.rest_fill) {  // caller's earlier pruned list
             const uint32_t* rr = a.rest_fill + node * a.rest_stride;
             const uint32_t rc = min(a.rest_fill_cnt[node], a.rest_stride);
@@ -407,7 +443,7 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
             uint32_t* rr = a.rest + node * a.rest_stride;
             uint32_t rw = 0;
             for (uint32_t j = 0; j < P && rw < a.rest_stride; ++j)
-                if (!s_keep[j]) rr[rw++] = s_ids[j];
+                if (!s_keep[j]) rr[rw++] = s_ids[j] >> 1;
             a.rest_cnt[node] = rw;
         }
     }

@@ -132,6 +132,8 @@ __global__ void __launch_bounds__(512) fast_search_kernel(SearchArgs a) {
                     }
             }
             u = __shfl_sync(kFull, u, owner);
+            if (a.path && pops < a.path_stride && lane == 0)
+                a.path[(size_t)qi * a.path_stride + pops] = u;
             ++pops;
 
             // qg.hpp:320-324: neighbours in list order, unvisited ones kept.
@@ -296,6 +298,9 @@ __global__ void __launch_bounds__(512) fast_search_kernel(SearchArgs a) {
                 pdo[j] = INF;
             }
         }
+        if (a.path)
+            for (uint32_t j = pops + lane; j < a.path_stride; j += 32)
+                a.path[(size_t)qi * a.path_stride + j] = kNoId;
         if (a.stats && lane == 0) {
             uint4 st = make_uint4(pops, calcs, 0u, P);
             *reinterpret_cast<uint4*>(a.stats + 4 * (size_t)qi) = st;

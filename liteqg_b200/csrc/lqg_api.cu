@@ -293,6 +293,8 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         a.flagged = w.d_flagged;
         a.vbits = t.visited_bits;
         a.ties_ok = b.ties_ok;
+        a.path = b.path;
+        a.path_stride = b.path_stride;
         int warps = plain ? 1 : (int)t.warps_per_block;
         int blocks = 1;
         if (!plain) {
@@ -757,7 +759,18 @@ lqg_status lqg_device_arrays(const lqg_index* ix, const uint32_t** nbrs, const u
 //              with its pruned candidates and, if still short, random ids.
 lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32_t num_iter,
                      uint64_t seed, uint32_t random_edges) {
+    return lqg_build_ex(ix, data, ef_build, num_iter, seed, random_edges, 1.0f, 0, 0);
+}
+
+lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uint32_t num_iter,
+                        uint64_t seed, uint32_t random_edges, float alpha, uint32_t path_take,
+                        uint32_t far_budget) {
     if (!ix || !data) return fail(LQG_ERR_ARG, "null argument");
+    if (!(alpha >= 1.0f && alpha <= 4.0f)) return fail(LQG_ERR_ARG, "alpha must be in [1, 4]");
+    if (path_take > 256) return fail(LQG_ERR_ARG, "path_take must be <= 256");
+    if (far_budget + random_edges >= ix->deg)
+        return fail(LQG_ERR_ARG, "far_budget + random_edges must be below degree_bound");
+    const float alpha2 = alpha * alpha;
     if (num_iter <= 1) return fail(LQG_ERR_ARG, "The number of iter for building qg should >= 3");
     if (ef_build == 0 || ef_build > kMaxEf) return fail(LQG_ERR_ARG, "EF must be in [1, 512]");
     if (ix->n <= ix->deg) return fail(LQG_ERR_ARG, "num_elements must exceed degree_bound");
@@ -789,15 +802,19 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
     uint32_t *d_kept = nullptr, *d_kept_cnt = nullptr, *d_rest = nullptr, *d_rest_cnt = nullptr;
     uint32_t *d_new = nullptr, *d_new_cnt = nullptr;
     lqg::ReverseWork rw{};
-    uint32_t *d_pool = nullptr, *d_k1 = nullptr;
+    uint32_t *d_pool = nullptr, *d_k1 = nullptr, *d_path = nullptr;
     float* d_pool_d = nullptr;
+    // the build searches run the fast kernel with ties resolved by insertion order
+    const lqg_tuning saved_tune = ix->tune;
+    ix->tune.mode = 1;
     auto cleanup = [&]() {
         dfree(d_x); dfree(d_c); if (d_work) cudaFree(d_work); d_work = nullptr;
         dfree(d_cent); dfree(d_best); dfree(d_kept); dfree(d_kept_cnt); dfree(d_rest);
         dfree(d_rest_cnt); dfree(d_new); dfree(d_new_cnt);
         dfree(rw.keys_in); dfree(rw.vals_in); dfree(rw.keys_out); dfree(rw.vals_out);
         dfree(rw.start); dfree(rw.end); if (rw.temp) cudaFree(rw.temp); rw.temp = nullptr;
-        dfree(d_pool); dfree(d_k1); dfree(d_pool_d);
+        dfree(d_pool); dfree(d_k1); dfree(d_pool_d); dfree(d_path);
+        ix->tune = saved_tune;
     };
     auto alloc = [&](auto*& p, size_t bytes) {
         if (cudaMalloc(&p, bytes) != cudaSuccess) {
@@ -820,7 +837,8 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
               alloc(rw.temp, (rw.temp_bytes = lqg::reverse_temp_bytes(n, deg)) + 256) &&
               alloc(d_new, n * deg * 4) && alloc(d_new_cnt, n * 4) &&
               alloc(d_pool, chunk * ef_build * 4) && alloc(d_pool_d, chunk * ef_build * 4) &&
-              alloc(d_k1, chunk * 4) && (ix->cstride == dim || alloc(d_c, n * dim));
+              alloc(d_k1, chunk * 4) && (ix->cstride == dim || alloc(d_c, n * dim)) &&
+              (path_take == 0 || alloc(d_path, chunk * path_take * 4));
     if (!ok) {
         cleanup();
         return fail(LQG_ERR_NOMEM, "device allocation for the build failed");
@@ -854,7 +872,7 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
         for (uint64_t c0 = 0; c0 < n; c0 += chunk) {
             const uint64_t m = std::min(chunk, n - c0);
             BatchSpec b{d_x + c0 * dim, (int64_t)m, nullptr, 1, nullptr, ef_build, d_k1, 1,
-                        d_pool, d_pool_d, ef_build, nullptr, st, 1};
+                        d_pool, d_pool_d, ef_build, nullptr, st, 1, d_path, path_take};
             if ((s = run_batch(ix, ix->ws, b, false)) != LQG_OK) {
                 cleanup();
                 return s;
@@ -878,6 +896,12 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
             a.rest = d_rest;
             a.rest_cnt = d_rest_cnt;
             a.rest_stride = rest_stride;
+            a.alpha2 = alpha2;
+            a.path = d_path;
+            a.path_stride = path_take;
+            a.path_take = path_take;
+            a.far_take = std::min<uint32_t>(path_take, 32);
+            a.far_budget = far_budget;
             LQG_BCUDA(lqg::launch_prune(a, m, st), "prune");
         }
         LQG_BCUDA(lqg::launch_reverse(d_kept, d_kept_cnt, n, deg, rw, st), "reverse edges");
@@ -897,6 +921,8 @@ lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32
         b.out_cnt = d_new_cnt;
         b.out_cap = deg - random_edges;
         b.fill = 1;
+        b.alpha2 = alpha2;
+        b.far_budget = far_budget;
         b.rest_fill = d_rest;
         b.rest_fill_cnt = d_rest_cnt;
         b.rest_stride = rest_stride;

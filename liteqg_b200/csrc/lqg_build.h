@@ -36,6 +36,16 @@ struct PruneArgs {
     uint32_t* rest;  // [n][rest_stride] pruned candidates, ascending (or null)
     uint32_t* rest_cnt;
     uint32_t rest_stride;
+    float alpha2;  // occlusion factor squared (squared distances): prune i if
+                   // alpha2 * d(j, i) < d(node, i); 1 = heuristic_prune
+    // search-path candidates (index build): [nodes][path_stride] popped ids,
+    // row 0 = node0; up to far_take of them beyond the nearest
+    // kPruneMax - far_take candidates also enter the prune
+    const uint32_t* path;
+    uint32_t path_stride, path_take, far_take;
+    // slots of a list that only candidates farther than 4x the nearest
+    // candidate's squared distance may take (long links)
+    uint32_t far_budget;
 };
 
 cudaError_t launch_sq8_encode(const float* x, uint64_t n, uint32_t dim, float* params,

@@ -123,6 +123,8 @@ struct BatchSpec {
     uint32_t* stats;
     cudaStream_t st;
     uint32_t ties_ok = 0;
+    uint32_t* path = nullptr;  // index build: popped ids per query (fast kernel)
+    uint32_t path_stride = 0;
 };
 
 template <typename T>

@@ -52,6 +52,8 @@ struct SearchArgs {
     uint32_t ties_ok;        // fast kernel: resolve equal distances by insertion
                              // order instead of handing the query to the exact
                              // kernel (index build only; not reference order)
+    uint32_t* path;          // fast kernel (index build): the first path_stride
+    uint32_t path_stride;    // popped ids of each query, padded with kNoId
 };
 
 // Exact kernel work areas, one per resident warp.

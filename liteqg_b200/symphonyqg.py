@@ -86,11 +86,15 @@ class Index:
         check(lib().lqg_set_ef(self.handle, int(EF)))
 
     def build_index(self, data, EF: int, num_iter: int = 3, num_thread: int = UINT_MAX,
-                    seed: int = 0, random_edges: int | None = None) -> None:
+                    seed: int = 0, random_edges: int | None = None,
+                    alpha: float = 1.0, path_take: int = 0, far_budget: int = 0) -> None:
         """Builds on the GPU (``num_thread`` is accepted and unused).
 
         ``random_edges`` slots of each neighbour list hold seeded random
-        long-range links (default ``degree_bound // 8``)."""
+        long-range links (default ``degree_bound // 8``); ``alpha`` >= 1 is
+        the prune's occlusion factor (1 = the reference's heuristic);
+        ``path_take`` search-path nodes join each node's candidates and
+        ``far_budget`` slots are held for long links (see lqg_build_ex)."""
         items = _as_f32(data)
         if items.ndim == 1:
             items = items.reshape(1, -1)
@@ -101,7 +105,8 @@ class Index:
         if num_iter <= 1:
             raise ValueError("The number of iter for building qg should >= 3")
         re = self.degree_bound // 8 if random_edges is None else int(random_edges)
-        check(lib().lqg_build(self.handle, _p(items), int(EF), int(num_iter), int(seed), re))
+        check(lib().lqg_build_ex(self.handle, _p(items), int(EF), int(num_iter), int(seed), re,
+                                 float(alpha), int(path_take), int(far_budget)))
 
     def search(self, query, k: int, ef=None, return_pool: bool = False,
                return_stats: bool = False):

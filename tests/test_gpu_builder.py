@@ -71,3 +71,35 @@ def test_build_rejects_bad_shapes():
         ix.build_index(np.zeros((99, 64), np.float32), 50)
     with pytest.raises(ValueError, match=">= 3"):
         ix.build_index(np.zeros((100, 64), np.float32), 50, num_iter=1)
+
+
+def test_build_search_path_links_reach_every_cluster():
+    """Clustered data (96 well-separated clusters): without search-path links
+    the clusters far from the entry point stay hard to reach; with them
+    (path_take, far_budget) recall at a small ef rises. The graph stays valid
+    and deterministic, and searching it stays exact against the oracle."""
+    import liteqg_b200
+
+    rng = np.random.default_rng(11)
+    n, dim, deg, nc = 24000, 48, 32, 96
+    cent = rng.uniform(0, 255, (nc, dim))
+    gen = lambda m: np.clip(np.rint(cent[rng.integers(0, nc, m)] + rng.normal(0, 12, (m, dim))),
+                            0, 255).astype(np.float32)
+    x, q = gen(n), gen(300)
+    gt = np.argsort(((q[:, None, :].astype(np.float64) - x[None].astype(np.float64)) ** 2).sum(-1), 1)[:, :10]
+    rec = {}
+    for name, kw in (("random", dict(random_edges=4)),
+                     ("path", dict(random_edges=4, path_take=64, far_budget=4))):
+        ix = liteqg_b200.Index("QG", "L2", n, dim, deg)
+        ix.build_index(x, 100, num_iter=3, **kw)
+        nb = ix.get_arrays()[2]
+        srt = np.sort(nb, axis=1)
+        assert not (srt[:, 1:] == srt[:, :-1]).any() and int(nb.max()) < n
+        _, (pid, _) = ix.search(q, 10, ef=32, return_pool=True)
+        rec[name] = _recall(pid, gt, 10)
+        if name == "path":
+            again = liteqg_b200.Index("QG", "L2", n, dim, deg)
+            again.build_index(x, 100, num_iter=3, **kw)
+            assert np.array_equal(again.get_arrays()[2], nb)
+    assert rec["path"] >= rec["random"], rec
+    assert rec["path"] >= 0.9, rec
