@@ -209,8 +209,8 @@ def load_peaks():
 
 
 def profile_traffic():
-    """DRAM bytes per query of the fast kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "fast_search_traffic.json")
+    """DRAM bytes per query of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "heap_search_traffic.json")
     try:
         with open(p) as f:
             return json.load(f)
@@ -473,7 +473,8 @@ def gpu_arm(args, w, name, rank, world, device):
 
     traffic = profile_traffic()
     traffic_launch = None
-    if traffic and traffic.get("workload") == name:
+    if (traffic and traffic.get("workload") == name and traffic.get("ef") == chosen
+            and mode == 2):
         traffic_launch = traffic["dram_bytes_per_query"] * nq
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": K,
