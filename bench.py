@@ -494,11 +494,14 @@ def gpu_arm(args, w, name, rank, world, device):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic_launch, "algorithmic_bytes_per_launch": bytes_launch,
                      "kernel_ms": statistics.mean(kern_ms),
-                     "kernel": ("fast_search_kernel + heap_search_kernel (tied queries)" if mode == 1
-                                else "heap_search_kernel")},
+                     "kernel": {1: "fast_search_kernel + heap_search_kernel (tied queries)",
+                                2: "heap_search_kernel",
+                                4: "split_search_kernel + rp_replay_kernel"}.get(mode, str(mode))},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": int(nq * dim * 4),
                 "d2h_bytes_per_step": int(nq * k * 4)},
-        "gpu_launches": 2 * K,
+        # kernels per batched step: fast + heap + exact (1), heap + exact (2),
+        # search + result replay + exact (3, 4); the L2 flush is torch's
+        "gpu_launches": {1: 3, 2: 2, 3: 3, 4: 3}.get(mode, 3) * K,
         "clocks": clk.summary(),
         "p50_ms": statistics.median(step_ms), "p99_ms": float(np.percentile(step_ms, 99)),
         **extra,

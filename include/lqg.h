@@ -200,8 +200,10 @@ LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
  *   mode            1: fast kernel for every query, heap kernel for the
  *                   queries whose distances tie; 2: heap kernel for every
  *                   query; 3: replay kernel for every query (sorted-pool
- *                   search warps, heap replay lanes; exact under ties)
- *   heap_warps      {1..8}: warps per block of the heap kernel
+ *                   search warps, heap replay lanes; exact under ties);
+ *                   4: split kernel for every query (exact search heap per
+ *                   warp, result heap replayed afterwards from a log)
+ *   heap_warps      {1..8}: warps per block of the heap and split kernels
  *   heap_scap       [256, 16384]: search-pool slots per query in shared
  *                   memory (heap and replay kernels; larger pools spill to
  *                   global memory, then to the global-memory kernel)

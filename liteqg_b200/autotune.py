@@ -1,7 +1,8 @@
 """Autotuner for the search kernels' launch shape and policy.
 
-Times a small grid of `lqg_tuning` settings (kernel mode, lanes per candidate,
-visited-cache size, warps per block, shared-memory search-pool slots) on a
+Times a small grid of `lqg_tuning` settings (kernel mode: 1 fast + heap for
+tied queries, 2 heap, 4 split; lanes per candidate, visited-cache size, warps
+per block, shared-memory search-pool slots) on a
 sample of the caller's queries with CUDA events, keeps the fastest, and caches
 the choice in a JSON file keyed on (N, D, degree, ef, k), so later runs on the
 same kind of index start from it. Every setting returns the same ids (the
@@ -18,6 +19,11 @@ DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "liteqg_b200", "
 
 # (mode, lanes_per_cand, visited_bits, warps_per_block, heap_warps, heap_scap)
 CANDIDATES = [
+    (4, 2, 10, 8, 4, 512),
+    (4, 4, 10, 8, 4, 512),
+    (4, 2, 11, 8, 4, 512),
+    (4, 2, 10, 8, 2, 512),
+    (4, 2, 10, 8, 4, 1024),
     (1, 4, 10, 8, 4, 1024),
     (2, 4, 10, 8, 4, 1024),
     (2, 4, 10, 8, 4, 512),

@@ -1,0 +1,105 @@
+// Warp-cooperative libstdc++ binary-heap steps on (id, distance bits) pairs,
+// shared by the heap and split search kernels. comp(x, y) is x.dist < y.dist
+// (symqglib/qg/qg.hpp:289-293); the search pool stores -distance.
+//   push: sift-up while comp(parent, value) (GCC bits/stl_heap.h
+//         __push_heap). The path from the new slot to the root is known and
+//         comp(parent, value) is monotone along it, so lane i loads the i-th
+//         ancestor, one ballot gives how far the value rises, and the shifted
+//         ancestors are written in one step.
+//   pop:  move the last element out, walk a hole from the root to a leaf
+//         along the larger child (the right one unless comp(right, left)),
+//         then sift the moved element up from there (__pop_heap /
+//         __adjust_heap). The walk is data dependent and runs on lane 0; the
+//         sift-up is the warp-parallel one.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lqg_kernels.cuh"
+
+namespace lqg {
+namespace heapops {
+
+__device__ __forceinline__ bool hless(uint2 x, uint2 y) {
+    return __uint_as_float(x.y) < __uint_as_float(y.y);
+}
+
+// A heap array: slots [0, cap) in shared memory, slots >= cap (the deepest
+// levels of a large search pool) in a per-warp global-memory area.
+struct HeapView {
+    uint2* s;
+    uint2* g;
+    uint32_t cap;
+    __device__ __forceinline__ uint2 get(uint32_t i) const { return i < cap ? s[i] : g[i - cap]; }
+    __device__ __forceinline__ void set(uint32_t i, uint2 v) const {
+        if (i < cap)
+            s[i] = v;
+        else
+            g[i - cap] = v;
+    }
+};
+
+// Sift-up of v from slot `hole` (libstdc++ __push_heap with top 0), all lanes.
+__device__ __forceinline__ void warp_sift_up(HeapView h, uint32_t hole, uint2 v, int lane) {
+    // ancestors of hole: ((hole + 1) >> i) - 1 for i = 1 .. depth
+    const uint32_t p1 = hole + 1;
+    const uint32_t depth = 31u - __clz(p1);  // floor(log2(hole + 1))
+    bool pred = false;
+    uint2 anc = make_uint2(0, 0);
+    if (lane >= 1 && (uint32_t)lane <= depth) {
+        anc = h.get((p1 >> lane) - 1u);
+        pred = hless(anc, v);
+    }
+    const unsigned m = __ballot_sync(kFull, pred);
+    // consecutive trues from level 1 upward: the loop of __push_heap stops
+    // at the first parent that is not less than the value
+    const uint32_t j = (uint32_t)(__ffs(~(m >> 1)) - 1);
+    // level l (1..j): its value moves down to level l - 1
+    if (lane >= 1 && (uint32_t)lane <= j) h.set((p1 >> (lane - 1)) - 1u, anc);
+    if (lane == 0) h.set((p1 >> j) - 1u, v);
+    __syncwarp();
+}
+
+__device__ __forceinline__ void warp_push(HeapView h, uint32_t& n, uint2 v, int lane) {
+    warp_sift_up(h, n, v, lane);
+    ++n;
+}
+
+// pop_heap + pop_back.
+__device__ __forceinline__ void warp_pop(HeapView h, uint32_t& n, int lane) {
+    const uint32_t size = n;
+    if (size > 1) {
+        uint32_t hole = 0;
+        uint2 v = make_uint2(0, 0);
+        if (lane == 0) {
+            const uint32_t len = size - 1;
+            v = h.get(len);
+            uint32_t second = 0;
+            while (second < (len - 1) / 2) {
+                second = 2 * (second + 1);
+                const uint2 r = h.get(second), l = h.get(second - 1);
+                if (hless(r, l)) {
+                    second--;
+                    h.set(hole, l);
+                } else {
+                    h.set(hole, r);
+                }
+                hole = second;
+            }
+            if ((len & 1u) == 0 && second == (len - 2) / 2) {
+                second = 2 * (second + 1);
+                h.set(hole, h.get(second - 1));
+                hole = second - 1;
+            }
+        }
+        __syncwarp();
+        hole = __shfl_sync(kFull, hole, 0);
+        v.x = __shfl_sync(kFull, v.x, 0);
+        v.y = __shfl_sync(kFull, v.y, 0);
+        warp_sift_up(h, hole, v, lane);
+    }
+    n = size - 1;
+}
+
+}  // namespace heapops
+}  // namespace lqg

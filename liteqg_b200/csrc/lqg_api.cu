@@ -203,11 +203,13 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     const bool heap_all = t.mode == 2;
     cudaError_t e;
 
-    if (t.mode == 3) {
-        // replay kernels over every query, in chunks whose result logs fit
-        // 1 GiB; spilled queries go to the exact kernel
+    if (t.mode == 3 || t.mode == 4) {
+        // replay (3) or split (4) kernel over every query, then the result
+        // replay pass, in chunks whose result logs fit 1 GiB; spilled queries
+        // go to the exact kernel
+        const bool split = t.mode == 4;
         const int RE = lqg::replay_pool_regs(b.ef0);
-        if (RE == 0) return fail(LQG_ERR_ARG, "ef too large for the replay kernel");
+        if (RE == 0) return fail(LQG_ERR_ARG, "ef too large for the replay kernels");
         lqg::ReplayArgs ra{};
         ra.rcap = (b.ef0 + 2u) & ~1u;
         ra.efcap = std::min(32u * (uint32_t)RE - 32u, ra.rcap - 1u);
@@ -221,19 +223,28 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         if ((s = grow(w.d_rlen, w.cap_rlen, (size_t)chunk)) != LQG_OK) return s;
         ra.rlog = w.d_rlog;
         ra.rlen = w.d_rlen;
-        int sw = plain ? 1 : (int)t.replay_warps;
-        while (sw > 1 && lqg::replay_smem_bytes(ix->dim, t.visited_bits, ra.scap, sw) > 227 * 1024)
-            --sw;
+        int sw = plain ? 1 : (int)(split ? t.heap_warps : t.replay_warps);
+        if (split) {
+            while (sw > 1 && lqg::split_smem_bytes(ix->dim, t.visited_bits, ra.scap, sw) > 227 * 1024)
+                --sw;
+        } else {
+            while (sw > 1 && lqg::replay_smem_bytes(ix->dim, t.visited_bits, ra.scap, sw) > 227 * 1024)
+                --sw;
+        }
         ra.swarps = (uint32_t)sw;
         SearchArgs h = base_args(ix, w, b);
         h.qhead = w.d_ctl + kCtlHeapHead;
         h.vbits = t.visited_bits;
+        auto launch = [&](const SearchArgs& c, int blocks, int* occ) {
+            return split ? lqg::launch_split(c, ra, RE, (int)t.lanes_per_cand, degw, sw, blocks, b.st, occ)
+                         : lqg::launch_replay(c, ra, RE, (int)t.lanes_per_cand, degw, blocks, b.st, occ);
+        };
         int rb = 1;
         if (!plain) {
             int occ = 0;
-            e = lqg::launch_replay(h, ra, RE, (int)t.lanes_per_cand, degw, 0, b.st, &occ);
+            e = launch(h, 0, &occ);
             if (e != cudaSuccess || occ <= 0)
-                return fail(LQG_ERR_ARG, "replay kernel cannot launch with this tuning");
+                return fail(LQG_ERR_ARG, "search kernel cannot launch with this tuning");
             rb = occ * ix->num_sms;
             const int64_t need = (chunk + sw - 1) / sw;
             if (need < rb) rb = (int)need;
@@ -244,7 +255,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             w.sp_global_slots = 0;
             if (cudaMalloc(&w.d_sp_global, slots * kHeapGlobalCap * sizeof(uint2)) != cudaSuccess) {
                 cudaGetLastError();
-                return fail(LQG_ERR_NOMEM, "replay kernel search-pool area allocation failed");
+                return fail(LQG_ERR_NOMEM, "search-pool area allocation failed");
             }
             w.sp_global_slots = slots;
         }
@@ -269,8 +280,8 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             if (c.stats) c.stats += off * 4;
             c.m = mc;
             const int cb = (int)std::min<int64_t>(rb, (mc + sw - 1) / sw);
-            e = lqg::launch_replay(c, ra, RE, (int)t.lanes_per_cand, degw, cb, b.st, nullptr);
-            if (e != cudaSuccess) return cuda_fail(e, "replay search launch");
+            e = launch(c, cb, nullptr);
+            if (e != cudaSuccess) return cuda_fail(e, "search launch");
             e = lqg::launch_rp_replay(c, ra, b.st);
             if (e != cudaSuccess) return cuda_fail(e, "result replay launch");
             SearchArgs x = c;
@@ -689,7 +700,7 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         n.blocks_per_sm = t->blocks_per_sm;
     }
     if (t->mode) {
-        if (t->mode > 3) return fail(LQG_ERR_ARG, "mode must be 1, 2 or 3");
+        if (t->mode > 4) return fail(LQG_ERR_ARG, "mode must be 1, 2, 3 or 4");
         n.mode = t->mode;
     }
     if (t->heap_warps) {
@@ -707,7 +718,9 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
     }
     if (n.mode == 3 && lqg::replay_smem_bytes(ix->dim, n.visited_bits, n.heap_scap, 1) > 227 * 1024)
         return fail(LQG_ERR_ARG, "replay kernel tuning needs more than 227 KB of shared memory");
-    if (n.mode != 3 &&
+    if (n.mode == 4 && lqg::split_smem_bytes(ix->dim, n.visited_bits, n.heap_scap, 1) > 227 * 1024)
+        return fail(LQG_ERR_ARG, "split kernel tuning needs more than 227 KB of shared memory");
+    if (n.mode <= 2 &&
         lqg::heap_smem_bytes(ix->dim, n.visited_bits, kMaxEf + 2, n.heap_scap, (int)n.heap_warps) >
         227 * 1024)
         return fail(LQG_ERR_ARG, "heap kernel tuning needs more than 227 KB of shared memory");

@@ -72,6 +72,11 @@ int replay_pool_regs(uint32_t ef_max);
 size_t replay_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t scap, int swarps);
 cudaError_t launch_replay(const SearchArgs& a, const ReplayArgs& ra, int E, int G, int degw,
                           int blocks, cudaStream_t st, int* occ);
+// Split kernel (split_kernel.cuh): exact search heap per warp, sorted
+// register array for the bound, result log for the replay pass.
+size_t split_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t scap, int warps);
+cudaError_t launch_split(const SearchArgs& a, const ReplayArgs& ra, int E, int G, int degw,
+                         int warps, int blocks, cudaStream_t st, int* occ);
 // Result-heap replay pass over a[0, m): one thread per query.
 cudaError_t launch_rp_replay(const SearchArgs& a, const ReplayArgs& ra, cudaStream_t st);
 

@@ -1,11 +1,15 @@
-"""GPU parity of the replay kernel (tuning mode 3) through the C ABI.
+"""GPU parity of the replay (tuning mode 3) and split (mode 4) kernels through the C ABI.
 
-Search warps run the sorted-pool form of the reference's loop and log every
-pool operation; replay lanes run the reference's two libstdc++ heaps from the
-log, check each step, and answer the search warps when equal distances make
-the heap layout decide. Bar: ids, FP32 pools and pop counts bit-exact against
-the reference's golden outputs and the oracle; queries only reach the exact
-global-memory kernel (stats flag 2) when a pool outgrows its capacity.
+Mode 3: search warps run the sorted-pool form of the reference's loop and log
+every search-pool operation; a replay lane runs the reference's libstdc++
+search heap from the log, checks each step, and answers when equal distances
+make the heap layout decide. Mode 4: each search warp runs the exact search
+heap itself and keeps only a sorted array for the bound. In both, the result
+heap is replayed afterwards from a per-query log by one thread per query,
+which checks every acceptance and writes the output. Bar: ids, FP32 pools and
+pop counts bit-exact against the reference's golden outputs and the oracle;
+queries only reach the exact global-memory kernel (stats flag 2) when a pool
+outgrows its capacity.
 """
 import numpy as np
 import pytest
@@ -22,10 +26,15 @@ def lqg():
     return liteqg_b200
 
 
-def open_index(lqg, g, **tune):
+@pytest.fixture(params=[3, 4], ids=["replay", "split"])
+def mode(request):
+    return request.param
+
+
+def open_index(lqg, g, mode, **tune):
     ix = lqg.Index("QG", "L2", g["n"], g["dim"], g["deg"])
     ix.load(g["path"])
-    ix.set_tuning(mode=3, **tune)
+    ix.set_tuning(mode=mode, **tune)
     return ix
 
 
@@ -33,10 +42,10 @@ def _oracle_for(g):
     return Oracle(read_index(g["path"], g["n"], g["dim"], g["deg"]))
 
 
-def test_replay_golden_every_ef_k(lqg, golden):
+def test_replay_golden_every_ef_k(lqg, golden, mode):
     """The reference's own outputs, every (ef, k) of the fixtures, batched and single."""
     for name, g in golden.items():
-        ix = open_index(lqg, g)
+        ix = open_index(lqg, g, mode)
         for (ef, k), want in g["expected"].items():
             ix.set_ef(ef)
             got = ix.search(g["queries"], k)
@@ -45,9 +54,9 @@ def test_replay_golden_every_ef_k(lqg, golden):
             assert np.array_equal(one, want[3]), (name, ef, k)
 
 
-def test_replay_pools_and_pops_bit_exact(lqg, golden):
+def test_replay_pools_and_pops_bit_exact(lqg, golden, mode):
     for name, g in golden.items():
-        ix = open_index(lqg, g)
+        ix = open_index(lqg, g, mode)
         o = _oracle_for(g)
         for ef in (10, 33, 100, 200, 480):
             want = o.search(g["queries"], 10, ef)
@@ -69,20 +78,20 @@ def test_replay_pools_and_pops_bit_exact(lqg, golden):
 
 @pytest.mark.parametrize("g_lanes,vbits,swarps,scap", [
     (4, 10, 15, 512), (2, 8, 4, 256), (8, 13, 1, 2048), (4, 9, 7, 1024), (2, 12, 15, 256)])
-def test_replay_tuning_does_not_change_results(lqg, golden, g_lanes, vbits, swarps, scap):
+def test_replay_tuning_does_not_change_results(lqg, golden, mode, g_lanes, vbits, swarps, scap):
     for name in ("mix128d64", "bin40"):
         g = golden[name]
-        ix = open_index(lqg, g, lanes_per_cand=g_lanes, visited_bits=vbits,
-                        replay_warps=swarps, heap_scap=scap)
+        ix = open_index(lqg, g, mode, lanes_per_cand=g_lanes, visited_bits=vbits,
+                        replay_warps=swarps, heap_warps=min(swarps, 8), heap_scap=scap)
         for ef, k in ((20, 10), (50, 50), (200, 10)):
             ix.set_ef(ef)
             assert np.array_equal(ix.search(g["queries"], k), g["expected"][(ef, k)]), (name, ef, k)
 
 
-def test_replay_tie_heavy_binary_vectors(lqg, golden):
+def test_replay_tie_heavy_binary_vectors(lqg, golden, mode):
     """Binary vectors: every query meets equal distances at the pop and the bound."""
     g = golden["bin40"]
-    ix = open_index(lqg, g)
+    ix = open_index(lqg, g, mode)
     o = _oracle_for(g)
     for ef in (20, 100, 200):
         want = o.search(g["queries"], 50, ef)
@@ -124,7 +133,7 @@ def _knn_graph(x, deg):
 
 
 @pytest.mark.parametrize("dim,deg,integer", [(128, 32, True), (96, 64, True), (64, 32, False)])
-def test_replay_larger_index_uneven_batch(lqg, tmp_path, dim, deg, integer):
+def test_replay_larger_index_uneven_batch(lqg, tmp_path, mode, dim, deg, integer):
     """12k nodes, exact-kNN graph; per-query ef in {1..512} and k in {1, 10, 100}."""
     from oracle.oracle import sq8_quantize
 
@@ -143,7 +152,7 @@ def test_replay_larger_index_uneven_batch(lqg, tmp_path, dim, deg, integer):
     write_index(path, arr)
     ix = lqg.Index("QG", "L2", n, dim, deg)
     ix.load(path)
-    ix.set_tuning(mode=3)
+    ix.set_tuning(mode=mode)
     o = Oracle(arr)
     q = gen(400)
     efq = rng.choice([1, 7, 32, 64, 100, 256, 512], size=len(q)).astype(np.uint32)
