@@ -19,11 +19,12 @@ DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "liteqg_b200", "
 
 # (mode, lanes_per_cand, visited_bits, warps_per_block, heap_warps, heap_scap)
 CANDIDATES = [
+    (4, 2, 10, 8, 4, 256),
     (4, 2, 10, 8, 4, 512),
     (4, 4, 10, 8, 4, 512),
+    (4, 4, 10, 8, 4, 256),
     (4, 2, 11, 8, 4, 512),
-    (4, 2, 10, 8, 2, 512),
-    (4, 2, 10, 8, 4, 1024),
+    (4, 2, 10, 8, 5, 256),
     (1, 4, 10, 8, 4, 1024),
     (2, 4, 10, 8, 4, 1024),
     (2, 4, 10, 8, 4, 512),

@@ -223,7 +223,8 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         if ((s = grow(w.d_rlen, w.cap_rlen, (size_t)chunk)) != LQG_OK) return s;
         ra.rlog = w.d_rlog;
         ra.rlen = w.d_rlen;
-        int sw = plain ? 1 : (int)(split ? t.heap_warps : t.replay_warps);
+        // split kernel blocks hold at most 5 warps (its 96-register budget)
+        int sw = plain ? 1 : (int)(split ? std::min(t.heap_warps, 5u) : t.replay_warps);
         if (split) {
             while (sw > 1 && lqg::split_smem_bytes(ix->dim, t.visited_bits, ra.scap, sw) > 227 * 1024)
                 --sw;

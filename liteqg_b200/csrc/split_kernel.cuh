@@ -51,8 +51,10 @@ __host__ __device__ inline size_t split_warp_bytes(uint32_t dim, uint32_t vbits,
     return 4 * dpad + 4 * ((size_t)1 << vbits) + kCandBytes + 8 * (size_t)scap;
 }
 
+// At most 5 warps per block and 96 registers per thread, so 20 warps (queries)
+// fit on an SM.
 template <int E, int G, int DEGW>
-__global__ void __launch_bounds__(256, 2) split_search_kernel(SearchArgs a, ReplayArgs ra) {
+__global__ void __launch_bounds__(160, 4) split_search_kernel(SearchArgs a, ReplayArgs ra) {
     using namespace heapops;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
