@@ -345,10 +345,10 @@ def gpu_arm(args, w, name, rank, world, device):
     pops, evals = stx[:, 0], stx[:, 1]
     exact_share = float((stf[:, 2] >= 1).mean())
     # launch shape and policy (fast+heap or heap-only, buffer sizes): autotuned
-    # on the first 4,000 queries; every setting gives the same ids
+    # on the whole batch; every setting gives the same ids
     from liteqg_b200 import autotune
 
-    tuned = autotune.tune(ix, queries[:4000], chosen, k, path=None, device=device)
+    tuned = autotune.tune(ix, queries, chosen, k, path=None, device=device)
     mode = tuned["mode"]
     mode_ms = {str(c): t for t, c in tuned["all"]}
     if args.profile:
@@ -496,12 +496,12 @@ def gpu_arm(args, w, name, rank, world, device):
                      "kernel_ms": statistics.mean(kern_ms),
                      "kernel": {1: "fast_search_kernel + heap_search_kernel (tied queries)",
                                 2: "heap_search_kernel",
-                                4: "split_search_kernel + rp_replay_kernel"}.get(mode, str(mode))},
+                                4: "split_search_kernel"}.get(mode, str(mode))},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": int(nq * dim * 4),
                 "d2h_bytes_per_step": int(nq * k * 4)},
         # kernels per batched step: fast + heap + exact (1), heap + exact (2),
-        # search + result replay + exact (3, 4); the L2 flush is torch's
-        "gpu_launches": {1: 3, 2: 2, 3: 3, 4: 3}.get(mode, 3) * K,
+        # replay + result replay + exact (3), split + exact (4); the L2 flush is torch's
+        "gpu_launches": {1: 3, 2: 2, 3: 3, 4: 2}.get(mode, 3) * K,
         "clocks": clk.summary(),
         "p50_ms": statistics.median(step_ms), "p99_ms": float(np.percentile(step_ms, 99)),
         **extra,

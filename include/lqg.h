@@ -208,7 +208,11 @@ LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
  *                   memory (heap and replay kernels; larger pools spill to
  *                   global memory, then to the global-memory kernel)
  *   replay_warps    {1..15}: search warps per block of the replay kernel
- *                   (plus one replay warp) */
+ *                   (plus one replay warp)
+ *   replay_all      mode 4: 1 sends every query through the checked result
+ *                   replay pass (0, the default: only queries whose output
+ *                   the heap layout decides); set on every call, not kept
+ *                   when 0 is passed */
 typedef struct {
     uint32_t lanes_per_cand;
     uint32_t visited_bits;
@@ -218,6 +222,7 @@ typedef struct {
     uint32_t heap_warps;
     uint32_t heap_scap;
     uint32_t replay_warps;
+    uint32_t replay_all;
 } lqg_tuning;
 
 LQG_API lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t);

@@ -69,6 +69,7 @@ class Tuning(C.Structure):
         ("heap_warps", C.c_uint32),
         ("heap_scap", C.c_uint32),
         ("replay_warps", C.c_uint32),
+        ("replay_all", C.c_uint32),
     ]
 
 

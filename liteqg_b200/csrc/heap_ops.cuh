@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "lqg_internal.h"
 #include "lqg_kernels.cuh"
 
 namespace lqg {
@@ -102,4 +103,65 @@ __device__ __forceinline__ void warp_pop(HeapView h, uint32_t& n, int lane) {
 }
 
 }  // namespace heapops
+
+// The result pool of query qi replayed from its log (qg.hpp:329-343) on the
+// heap rp (one warp): the logged accepted nodes in order, each checked
+// against the reference's acceptance test on this heap (size < ef or top >
+// distance) and the logged bound after it against rp.top(); then the output:
+// the first k pops (results[k-1-j] = j-th pop) and, if asked, the whole pool
+// in ascending order. The log is read 32 entries per coalesced load. Returns
+// false (nothing written) when a check fails.
+__device__ __forceinline__ bool replay_result(const SearchArgs& a, const ReplayArgs& ra,
+                                              int64_t qi, uint32_t len, const heapops::HeapView rp,
+                                              int lane) {
+    using namespace heapops;
+    const uint32_t efq = a.efq ? a.efq[qi] : a.ef0;
+    const uint32_t ef = min(max(efq, 1u), ra.efcap);
+    const uint32_t k = min(a.kq ? a.kq[qi] : a.k0, a.kstride);
+    const uint4* lg = ra.rlog + (size_t)qi * ra.rlog_cap;
+    uint32_t n = 0;
+    bool ok = len > 0 && len <= ra.rlog_cap;
+    for (uint32_t b = 0; ok && b < len; b += 32) {
+        const uint4 mine = b + lane < len ? __ldcs(lg + b + lane) : make_uint4(0, 0, 0, 0);
+        const uint32_t cnt = min(32u, len - b);
+        for (uint32_t j = 0; j < cnt; ++j) {
+            const uint32_t id = __shfl_sync(kFull, mine.x, j);
+            const uint32_t yb = __shfl_sync(kFull, mine.y, j);
+            const uint32_t lb = __shfl_sync(kFull, mine.z, j);
+            if (!(n < ef || __uint_as_float(rp.get(0).y) > __uint_as_float(yb))) {
+                ok = false;
+                break;
+            }
+            warp_push(rp, n, make_uint2(id, yb), lane);
+            if (n > ef) warp_pop(rp, n, lane);
+            if (rp.get(0).y != lb) {
+                ok = false;
+                break;
+            }
+        }
+    }
+    if (!ok) return false;
+    const uint32_t P = n, kk = min(k, P);
+    uint32_t* out = a.ids + (size_t)qi * a.kstride;
+    for (uint32_t x = lane; x < k - kk; x += 32) out[x] = kNoId;
+    if (a.pool_ids)
+        for (uint32_t x = P + lane; x < a.pstride; x += 32) {
+            a.pool_ids[(size_t)qi * a.pstride + x] = kNoId;
+            a.pool_d[(size_t)qi * a.pstride + x] = __int_as_float(0x7f800000);
+        }
+    const uint32_t ex = a.pool_ids ? P : kk;
+    for (uint32_t j = 0; j < ex; ++j) {
+        const uint2 t = rp.get(0);
+        if (lane == 0) {
+            if (j < kk) out[k - 1 - j] = t.x;
+            if (a.pool_ids && P - 1 - j < a.pstride) {
+                a.pool_ids[(size_t)qi * a.pstride + (P - 1 - j)] = t.x;
+                a.pool_d[(size_t)qi * a.pstride + (P - 1 - j)] = __uint_as_float(t.y);
+            }
+        }
+        warp_pop(rp, n, lane);
+    }
+    return true;
+}
+
 }  // namespace lqg

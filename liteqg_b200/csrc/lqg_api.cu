@@ -217,6 +217,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         ra.spill = w.d_spill;
         ra.nspill = w.d_ctl + kCtlSpilled;
         ra.rlog_cap = std::max(1024u, 16u * b.ef0);
+        ra.replay_all = t.replay_all;
         const int64_t chunk = std::min<int64_t>(
             b.m, std::max<int64_t>(1024, (int64_t(1) << 30) / ((int64_t)ra.rlog_cap * 16)));
         if ((s = grow(w.d_rlog, w.cap_rlog, (size_t)chunk * ra.rlog_cap)) != LQG_OK) return s;
@@ -283,8 +284,11 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             const int cb = (int)std::min<int64_t>(rb, (mc + sw - 1) / sw);
             e = launch(c, cb, nullptr);
             if (e != cudaSuccess) return cuda_fail(e, "search launch");
-            e = lqg::launch_rp_replay(c, ra, b.st);
-            if (e != cudaSuccess) return cuda_fail(e, "result replay launch");
+            if (!split || ra.replay_all ||
+                !lqg::split_replays_in_place_host(t.visited_bits, ra.scap, ra.rcap)) {
+                e = lqg::launch_rp_replay(c, ra, b.st);
+                if (e != cudaSuccess) return cuda_fail(e, "result replay launch");
+            }
             SearchArgs x = c;
             x.qlist = w.d_spill;
             x.nlist = w.d_ctl + kCtlSpilled;
@@ -713,6 +717,7 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
             return fail(LQG_ERR_ARG, "heap_scap must be in [256, 16384]");
         n.heap_scap = t->heap_scap;
     }
+    n.replay_all = t->replay_all ? 1u : 0u;
     if (t->replay_warps) {
         if (t->replay_warps > 15) return fail(LQG_ERR_ARG, "replay_warps must be in [1, 15]");
         n.replay_warps = t->replay_warps;

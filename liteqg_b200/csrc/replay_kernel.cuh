@@ -35,7 +35,7 @@
 // last element), checks that each POP is sp.top() and that at END the
 // reference's loop would stop, and answers the tie questions.
 //
-// rp_replay_kernel (one thread per query, after the search): replays the
+// rp_replay_kernel (one warp per query, after the search): replays the
 // result log on a result heap laid out as libstdc++ leaves it, checks each
 // accepted node against the reference's acceptance test on that heap and the
 // logged bound against rp.top(), and writes the output by popping rp

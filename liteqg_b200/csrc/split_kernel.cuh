@@ -12,10 +12,12 @@
 // it is the largest accepted one). The warp keeps the accepted nodes at or
 // below the bound sorted in registers (E entries per lane) for that, and
 // appends every accepted node, in order, to the query's result log in HBM
-// (id, distance, bound after). rp_replay_kernel (replay_launch.cu) then
-// replays the log on a result heap laid out exactly as libstdc++ leaves it,
-// checks every acceptance against the reference's test on that heap and the
-// logged bound against rp.top(), and writes the output (qg.hpp:340-343).
+// (id, distance, bound after). When the output does not depend on how equal
+// distances sit in rp (below), the warp writes it from the sorted array;
+// otherwise rp_replay_kernel (replay_launch.cu) replays the log on a result
+// heap laid out exactly as libstdc++ leaves it, checks every acceptance
+// against the reference's test on that heap and the logged bound against
+// rp.top(), and writes the output (qg.hpp:340-343).
 //
 // Visited set: the direct-mapped cache of evaluated ids in shared memory. It
 // may forget an id, never invents one. A forgotten node that is evaluated
@@ -49,6 +51,12 @@ __device__ __forceinline__ float spool_at(const float (&pd)[E], uint32_t pos) {
 __host__ __device__ inline size_t split_warp_bytes(uint32_t dim, uint32_t vbits, uint32_t scap) {
     const size_t dpad = (dim + 15u) & ~15u;
     return 4 * dpad + 4 * ((size_t)1 << vbits) + kCandBytes + 8 * (size_t)scap;
+}
+
+// After a search, a warp's visited cache, candidates and search heap can
+// hold a result heap of rcap slots.
+__host__ __device__ inline bool split_replays_in_place(uint32_t vbits, uint32_t scap, uint32_t rcap) {
+    return 4 * ((size_t)1 << vbits) + kCandBytes + 8 * (size_t)scap >= 8 * (size_t)rcap;
 }
 
 // At most 5 warps per block and 96 registers per thread, so 20 warps (queries)
@@ -237,14 +245,64 @@ __global__ void __launch_bounds__(160, 4) split_search_kernel(SearchArgs a, Repl
             }
         }
 
+        // Output (qg.hpp:340-343). rp pops come out in descending distance;
+        // only equal distances make the heap layout decide. So when the
+        // sorted array holds exactly rp (no ties beyond the ef-th entry) and
+        // the popped entries (the worst k and the one after them, or the
+        // whole pool when it is returned) have distinct distances, the output
+        // is read off the array; otherwise the result replay pass computes it.
+        const uint32_t P = min(acc_n, ef);
+        bool direct = false;
+        if (!fail && !ra.replay_all) {
+            const uint32_t k = min(a.kq ? a.kq[qi] : a.k0, a.kstride);
+            const uint32_t kk = min(k, P);
+            const uint32_t lo = a.pool_ids ? 0u : (P > kk ? P - kk - 1 : 0u);
+            const float nx0 = __shfl_down_sync(kFull, pd[0], 1);
+            uint32_t vc = 0;
+            bool tie = false;
+#pragma unroll
+            for (int t = 0; t < E; ++t) {
+                const uint32_t pos = (uint32_t)lane * E + t;
+                vc += pd[t] < INF ? 1u : 0u;
+                const float nxt = t + 1 < E ? pd[t + 1 < E ? t + 1 : 0] : nx0;
+                if (pos >= lo && pos + 1 < P && pd[t] == nxt) tie = true;
+            }
+            direct = __reduce_add_sync(kFull, vc) == P && !__any_sync(kFull, tie);
+            if (direct) {
+                uint32_t* out = a.ids + (size_t)qi * a.kstride;
+                for (uint32_t x = lane; x < k - kk; x += 32) out[x] = kNoId;
+#pragma unroll
+                for (int t = 0; t < E; ++t) {
+                    const uint32_t pos = (uint32_t)lane * E + t;
+                    if (pos < P && pos + kk >= P) out[pos + k - P] = pi[t];
+                    if (a.pool_ids && pos < P && pos < a.pstride) {
+                        a.pool_ids[(size_t)qi * a.pstride + pos] = pi[t];
+                        a.pool_d[(size_t)qi * a.pstride + pos] = pd[t];
+                    }
+                }
+                if (a.pool_ids)
+                    for (uint32_t x = P + lane; x < a.pstride; x += 32) {
+                        a.pool_ids[(size_t)qi * a.pstride + x] = kNoId;
+                        a.pool_d[(size_t)qi * a.pstride + x] = INF;
+                    }
+            }
+        }
+        // an output the heap layout decides: replay rp here, in this warp's
+        // shared memory (its visited cache, candidates and search heap are
+        // free now), else in the result replay pass
+        if (!fail && !direct && !ra.replay_all && split_replays_in_place(vbits, ra.scap, ra.rcap)) {
+            __syncwarp();
+            const HeapView rph{reinterpret_cast<uint2*>(vis), nullptr, ra.rcap};
+            fail = !replay_result(a, ra, qi, acc_n, rph, lane);
+            direct = !fail;
+        }
         if (lane == 0) {
-            ra.rlen[qi] = fail ? kNoId : acc_n;
+            ra.rlen[qi] = fail ? kNoId : (direct ? kRlenDone : acc_n);
             if (fail) {
                 const uint32_t i = atomicAdd(ra.nspill, 1u);
                 ra.spill[i] = (int32_t)qi;
             }
             if (a.stats) {
-                const uint32_t P = min(acc_n, ef);
                 *reinterpret_cast<uint4*>(a.stats + 4 * (size_t)qi) =
                     make_uint4(pops, calcs, 0u, P);
             }

@@ -13,6 +13,10 @@ LQG_SPLIT_EXTERN(9)
 LQG_SPLIT_EXTERN(17)
 #undef LQG_SPLIT_EXTERN
 
+bool split_replays_in_place_host(uint32_t vbits, uint32_t scap, uint32_t rcap) {
+    return split_replays_in_place(vbits, scap, rcap);
+}
+
 size_t split_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t scap, int warps) {
     const size_t dpad = (dim + 15u) & ~15u;
     return 8 * dpad + (size_t)warps * split_warp_bytes(dim, vbits, scap);

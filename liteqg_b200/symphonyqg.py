@@ -195,9 +195,9 @@ class Index:
 
     def set_tuning(self, lanes_per_cand=0, visited_bits=0, warps_per_block=0,
                    blocks_per_sm=0, mode=0, heap_warps=0, heap_scap=0,
-                   replay_warps=0) -> None:
+                   replay_warps=0, replay_all=0) -> None:
         t = Tuning(lanes_per_cand, visited_bits, warps_per_block, blocks_per_sm, mode,
-                   heap_warps, heap_scap, replay_warps)
+                   heap_warps, heap_scap, replay_warps, replay_all)
         check(lib().lqg_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:

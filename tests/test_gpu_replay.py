@@ -5,7 +5,7 @@ every search-pool operation; a replay lane runs the reference's libstdc++
 search heap from the log, checks each step, and answers when equal distances
 make the heap layout decide. Mode 4: each search warp runs the exact search
 heap itself and keeps only a sorted array for the bound. In both, the result
-heap is replayed afterwards from a per-query log by one thread per query,
+heap is replayed afterwards from a per-query log by one warp per query,
 which checks every acceptance and writes the output. Bar: ids, FP32 pools and
 pop counts bit-exact against the reference's golden outputs and the oracle;
 queries only reach the exact global-memory kernel (stats flag 2) when a pool
@@ -26,7 +26,10 @@ def lqg():
     return liteqg_b200
 
 
-@pytest.fixture(params=[3, 4], ids=["replay", "split"])
+# (tuning mode, replay_all): the split kernel writes unambiguous outputs from
+# its sorted array; replay_all=1 sends every query through the checked result
+# replay pass instead, so both paths are covered.
+@pytest.fixture(params=[(3, 0), (4, 0), (4, 1)], ids=["replay", "split", "split-replay-all"])
 def mode(request):
     return request.param
 
@@ -34,7 +37,7 @@ def mode(request):
 def open_index(lqg, g, mode, **tune):
     ix = lqg.Index("QG", "L2", g["n"], g["dim"], g["deg"])
     ix.load(g["path"])
-    ix.set_tuning(mode=mode, **tune)
+    ix.set_tuning(mode=mode[0], replay_all=mode[1], **tune)
     return ix
 
 
@@ -82,7 +85,7 @@ def test_replay_tuning_does_not_change_results(lqg, golden, mode, g_lanes, vbits
     for name in ("mix128d64", "bin40"):
         g = golden[name]
         ix = open_index(lqg, g, mode, lanes_per_cand=g_lanes, visited_bits=vbits,
-                        replay_warps=swarps, heap_warps=min(swarps, 8), heap_scap=scap)
+                        replay_warps=swarps, heap_warps=min(swarps, 5), heap_scap=scap)
         for ef, k in ((20, 10), (50, 50), (200, 10)):
             ix.set_ef(ef)
             assert np.array_equal(ix.search(g["queries"], k), g["expected"][(ef, k)]), (name, ef, k)
@@ -152,7 +155,7 @@ def test_replay_larger_index_uneven_batch(lqg, tmp_path, mode, dim, deg, integer
     write_index(path, arr)
     ix = lqg.Index("QG", "L2", n, dim, deg)
     ix.load(path)
-    ix.set_tuning(mode=mode)
+    ix.set_tuning(mode=mode[0], replay_all=mode[1])
     o = Oracle(arr)
     q = gen(400)
     efq = rng.choice([1, 7, 32, 64, 100, 256, 512], size=len(q)).astype(np.uint32)
