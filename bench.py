@@ -298,6 +298,7 @@ def gpu_arm(args, w, name, rank, world, device):
 
     import liteqg_b200
     from liteqg_b200._capi import check, lib
+    from liteqg_b200.replicas import max_over_ranks
 
     torch.cuda.set_device(device)
     t0 = time.perf_counter()
@@ -396,11 +397,7 @@ def gpu_arm(args, w, name, rank, world, device):
     log(f"[rank {rank}] timed loop done {time.perf_counter() - t0:.1f}s")
     step_ms = [a.elapsed_time(b) for a, b in ev]
     kern_ms = [a.elapsed_time(b) for a, b in kev]
-    total_s = sum(step_ms) / 1e3
-    if world > 1:
-        t = torch.tensor([total_s], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_s = float(t.item())
+    total_s = max_over_ranks(sum(step_ms) / 1e3, device=dev)
     value = world * nq * K / total_s
     kern_avg_s = statistics.mean(kern_ms) / 1e3
     achieved = bytes_launch / kern_avg_s / 1e9
@@ -421,11 +418,7 @@ def gpu_arm(args, w, name, rank, world, device):
         b.synchronize()
         if i >= max(3, args.warmup):
             e2e_ms.append(a.elapsed_time(b))
-    e2e_total = sum(e2e_ms) / 1e3
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(sum(e2e_ms) / 1e3, device=dev)
     e2e = world * nq * K / e2e_total
     e2e_ok = bool((ids_pin.numpy() == ids.cpu().numpy()).all())
 
