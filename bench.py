@@ -58,6 +58,17 @@ WORKLOADS = {
     "small-100k64": dict(n=100_000, dim=64, gen="uniform", deg=32, efb=200, iters=3,
                          random_edges=4, path_take=64, far_budget=4, nq=1000, k=10,
                          efs=(20, 40, 60, 100, 200), k_extra=100),
+    # uneven batch, high dimension (per-query ef and k;
+    # CUDA-graph replay timed beside the eager launch)
+    "uneven-1m960": dict(n=1_000_000, dim=960, gen="gauss_mixture", clusters=256, sigma=0.3,
+                         deg=64, efb=400, iters=3, random_edges=8, path_take=64, far_budget=8,
+                         nq=4096, kind="uneven", ef_choices=(32, 64, 128, 256, 512),
+                         k_choices=(1, 10, 100)),
+    # serving loop, open-loop Poisson arrivals
+    "serving-10m96": dict(n=10_000_000, dim=96, gen="gauss_mixture", clusters=4096, sigma=0.25,
+                          deg=32, efb=300, iters=3, random_edges=8, path_take=64, far_budget=8,
+                          nq=400_000, kind="serving", rates=(20_000, 100_000, 500_000),
+                          k_choices=(10, 100), ef_choices=(50, 100, 200, 500), seconds=4.0),
 }
 
 
@@ -72,6 +83,16 @@ def gen_data(w, which: str, rank: int = 0):
     if w["gen"] == "uniform":
         rng = np.random.default_rng(0 if which == "base" else 1 + 1000 * rank)
         return rng.random((n, w["dim"]), dtype=np.float32)
+    if w["gen"] == "gauss_mixture":  # centre entries N(0, 1), isotropic sigma, float
+        centres = np.random.default_rng(0).normal(0.0, 1.0, (w["clusters"], w["dim"]))
+        rng = np.random.default_rng(100 if which == "base" else 1 + 1000 * rank)
+        out = np.empty((n, w["dim"]), dtype=np.float32)
+        step = 1 << 17
+        for s in range(0, n, step):
+            m = min(step, n - s)
+            lab = rng.integers(0, w["clusters"], m)
+            out[s:s + m] = centres[lab] + rng.normal(0.0, w["sigma"], (m, w["dim"]))
+        return out
     centres = np.random.default_rng(0).uniform(w["lo"], w["hi"], (w["clusters"], w["dim"]))
     rng = np.random.default_rng(100 if which == "base" else 1 + 1000 * rank)
     out = np.empty((n, w["dim"]), dtype=np.float32)
@@ -118,7 +139,7 @@ def ground_truth(name, w, base, queries, device, rank):
     """FP64 brute-force top-100 ids per query (GPU, chunked), cached."""
     import torch
 
-    path = os.path.join(cache_dir(), key_of(name, w) + f".gt{rank}.npy")
+    path = os.path.join(cache_dir(), key_of(name, w) + f".gt{rank}-{len(queries)}.npy")
     if os.path.exists(path):
         return np.load(path)
     dev = torch.device("cuda", device)
@@ -126,8 +147,9 @@ def ground_truth(name, w, base, queries, device, rank):
     nb = (xb * xb).sum(1)
     kk = 100
     out = np.empty((len(queries), kk), np.int64)
-    for s in range(0, len(queries), 1024):
-        q = torch.from_numpy(queries[s:s + 1024]).to(dev, torch.float64)
+    qc = max(16, min(1024, (4 << 30) // (8 * len(base))))  # distance block <= 4 GiB
+    for s in range(0, len(queries), qc):
+        q = torch.from_numpy(queries[s:s + qc]).to(dev, torch.float64)
         d = nb[None, :] - 2.0 * (q @ xb.T) + (q * q).sum(1)[:, None]
         out[s:s + len(q)] = torch.topk(d, kk, dim=1, largest=False).indices.cpu().numpy()
     del xb
@@ -506,6 +528,173 @@ def gpu_arm(args, w, name, rank, world, device):
     ix.close()
 
 
+def _timed(fn, reps, flush, stream):
+    """Mean device ms of fn over reps, L2 flushed before each (CUDA events)."""
+    import torch
+
+    tot = 0.0
+    for i in range(reps):
+        flush.fill_(i & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        tot += a.elapsed_time(b)
+    return tot / reps
+
+
+def uneven_arm(args, w, name, device):
+    """one batch with per-query ef and k, eager and as a CUDA graph."""
+    import torch
+
+    import liteqg_b200
+
+    torch.cuda.set_device(device)
+    t0 = time.perf_counter()
+    base = gen_data(w, "base")
+    queries = gen_data(w, "query")
+    path, t_build = get_index_file(name, w, base, device)
+    gt = ground_truth(name, w, base, queries, device, 0)
+    del base
+    log(f"[uneven] index + gt ready {time.perf_counter() - t0:.1f}s (build {t_build:.1f}s)")
+    n, dim, deg, nq = w["n"], w["dim"], w["deg"], w["nq"]
+    ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
+    ix.load(path)
+    rng = np.random.default_rng(2)
+    efq = rng.choice(w["ef_choices"], nq).astype(np.uint32)
+    kq = rng.choice(w["k_choices"], nq).astype(np.uint32)
+    kmax, efmax = int(kq.max()), int(efq.max())
+    # recall: best-10 of each query's pool (untimed)
+    _, (pid, _) = ix.search(queries, 10, ef=efq, return_pool=True)
+    rec_by_ef = {int(e): recall_at(pid[efq == e], gt[efq == e], 10) for e in w["ef_choices"]}
+    dev = torch.device("cuda", device)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    q_dev = torch.from_numpy(queries).to(dev)
+    ids = torch.empty((nq, kmax), dtype=torch.int32, device=dev)
+    e_dev = torch.from_numpy(efq.view(np.int32)).to(dev)
+    k_dev = torch.from_numpy(kq.view(np.int32)).to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        ix.search_device(q_dev.data_ptr(), nq, 0, ids.data_ptr(), kmax, ef=efmax,
+                         ef_ptr=e_dev.data_ptr(), k_ptr=k_dev.data_ptr(), stream=sh)
+
+    best = None
+    for mode, g in ((4, 4), (4, 8), (2, 4), (1, 4)):
+        ix.set_tuning(mode=mode, lanes_per_cand=g, heap_warps=4, heap_scap=512, visited_bits=10)
+        for _ in range(2):
+            step()
+        ix.stream_status(sh)
+        ms = _timed(step, 5, flush, stream)
+        log(f"[uneven] mode {mode} G {g}: {ms:.2f} ms")
+        if best is None or ms < best[0]:
+            best = (ms, mode, g)
+    ix.set_tuning(mode=best[1], lanes_per_cand=best[2], heap_warps=4, heap_scap=512,
+                  visited_bits=10)
+    for _ in range(max(3, args.warmup)):
+        step()
+    ix.stream_status(sh)
+    K = max(1, min(args.steps, 50))
+    eager_ms = _timed(step, K, flush, stream)
+    eager_ids = ids.cpu().numpy().copy()
+    # the same batch captured in a CUDA graph
+    s2 = torch.cuda.Stream(dev)
+    s2.wait_stream(stream)
+    with torch.cuda.stream(s2):
+        ix.search_device(q_dev.data_ptr(), nq, 0, ids.data_ptr(), kmax, ef=efmax,
+                         ef_ptr=e_dev.data_ptr(), k_ptr=k_dev.data_ptr(), stream=s2.cuda_stream)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=s2):
+            ix.search_device(q_dev.data_ptr(), nq, 0, ids.data_ptr(), kmax, ef=efmax,
+                             ef_ptr=e_dev.data_ptr(), k_ptr=k_dev.data_ptr(),
+                             stream=s2.cuda_stream)
+    torch.cuda.synchronize(dev)
+    graph_ms = _timed(graph.replay, K, flush, stream)
+    graph_ok = bool((ids.cpu().numpy() == eager_ids).all())
+    del graph
+    line = {
+        "metric": METRIC, "value": nq / (eager_ms / 1e3), "unit": "queries/s", "n_gpus": 1,
+        "steps": K, "warmup": max(3, args.warmup), "ms_per_step": eager_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']}, {nq} queries, "
+                               f"per-query ef from {list(w['ef_choices'])}, k from "
+                               f"{list(w['k_choices'])} (seed 2)",
+                   "recall_at_10_pool_by_ef": rec_by_ef, "mode": best[1], "lanes_per_cand": best[2],
+                   "l2": "flushed between steps (256 MiB write)"},
+        "graph_qps": nq / (graph_ms / 1e3), "graph_ids_equal": graph_ok,
+        "gpu_launches": {1: 3, 2: 2, 4: 2}.get(best[1], 3) * K,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def serving_arm(args, w, name, device):
+    """open-loop Poisson arrivals through the serving loop."""
+    import torch
+
+    import liteqg_b200
+    from liteqg_b200.serving import Server
+
+    torch.cuda.set_device(device)
+    t0 = time.perf_counter()
+    base = gen_data(w, "base")
+    queries = gen_data(w, "query")
+    path, t_build = get_index_file(name, w, base, device)
+    sample = queries[:2000]
+    gt = ground_truth(name, w, base, sample, device, 0)
+    del base
+    log(f"[serving] index + gt ready {time.perf_counter() - t0:.1f}s (build {t_build:.1f}s)")
+    n, dim, deg = w["n"], w["dim"], w["deg"]
+    ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
+    ix.load(path)
+    ix.set_tuning(mode=4, lanes_per_cand=4, heap_warps=4, heap_scap=512, visited_bits=10)
+    rec = {}
+    for ef in w["ef_choices"]:
+        _, (pid, _) = ix.search(sample, 10, ef=ef, return_pool=True)
+        rec[int(ef)] = recall_at(pid, gt, 10)
+    rng = np.random.default_rng(3)
+    rows = []
+    with Server(ix, streams=4, max_k=max(w["k_choices"]), max_ef=max(w["ef_choices"])) as srv:
+        for rate in w["rates"]:
+            m = int(min(len(queries), rate * w["seconds"]))
+            arrivals = np.cumsum(rng.exponential(1e6 / rate, m))
+            ks = rng.choice(w["k_choices"], m).astype(np.uint32)
+            efs = rng.choice(w["ef_choices"], m).astype(np.uint32)
+            srv.reset_stats()
+            t = time.perf_counter()
+            _, lat = srv.replay(queries[:m], ks, efs, arrivals)
+            wall = time.perf_counter() - t
+            st = srv.stats()
+            rows.append({"offered_qps": rate, "requests": m, "achieved_qps": m / wall,
+                         "p50_ms": float(np.percentile(lat, 50)) / 1e3,
+                         "p99_ms": float(np.percentile(lat, 99)) / 1e3,
+                         "mean_batch": st["mean_batch"]})
+            log(f"[serving] {rows[-1]}")
+    # plain path: one query per call
+    lat = []
+    for i in range(520):
+        t = time.perf_counter()
+        ix.search(queries[i], 10, ef=100)
+        if i >= 20:
+            lat.append(time.perf_counter() - t)
+    line = {
+        "metric": METRIC, "value": max(r["achieved_qps"] for r in rows), "unit": "queries/s",
+        "n_gpus": 1, "steps": len(rows), "warmup": 0, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']}, open-loop "
+                               f"Poisson arrivals, k from {list(w['k_choices'])}, ef from "
+                               f"{list(w['ef_choices'])}", "recall_at_10_pool_by_ef": rec,
+                   "server": {"streams": 4}},
+        "serving": rows,
+        "plain_qps": len(lat) / sum(lat), "plain_p50_ms": 1e3 * float(np.percentile(lat, 50)),
+        "plain_p99_ms": 1e3 * float(np.percentile(lat, 99)),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -534,7 +723,12 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                              device_id=torch.device("cuda", local))
     try:
-        gpu_arm(args, w, args.workload, rank, world, local)
+        if w.get("kind") == "uneven":
+            uneven_arm(args, w, args.workload, local)
+        elif w.get("kind") == "serving":
+            serving_arm(args, w, args.workload, local)
+        else:
+            gpu_arm(args, w, args.workload, rank, world, local)
     finally:
         if world > 1:
             import torch
