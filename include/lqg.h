@@ -105,10 +105,22 @@ LQG_API lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build
  *   far_budget   slots of each list that only candidates farther than twice
  *                the nearest candidate's distance may take.
  * With reverse edges these become routes from the entry region into every
- * cluster of clustered data. */
+ * cluster of clustered data.
+ *   pair_kernel  candidate-to-candidate distances of the prune: 0 FP32 on the
+ *                CUDA cores; 1 BF16 Gram matrices on the tensor cores
+ *                (tcgen05, FP32 accumulation in tensor memory) with every
+ *                prune decision near its threshold re-checked in FP32, which
+ *                gives the same graph as 0.
+ *   report       optional: prune kernel time and FP32 re-checks of the build. */
+typedef struct {
+    double prune_ms;    /* all prune launches (CUDA events) */
+    double build_ms;    /* the whole build on the device */
+    uint64_t rechecks;  /* pair_kernel 1: decisions re-checked in FP32 */
+} lqg_build_report;
 LQG_API lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build,
                                 uint32_t num_iter, uint64_t seed, uint32_t random_edges,
-                                float alpha, uint32_t path_take, uint32_t far_budget);
+                                float alpha, uint32_t path_take, uint32_t far_budget,
+                                uint32_t pair_kernel, lqg_build_report* report);
 
 /* Index.set_ef: symqglib/qg/qg.hpp:226-230. ef in [1, 512]. */
 LQG_API lqg_status lqg_set_ef(lqg_index* ix, uint32_t ef);

@@ -33,7 +33,7 @@ SIGNATURES = {
     "lqg_set_ef": (C.c_int, [_vp, C.c_uint32]),
     "lqg_build": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32]),
     "lqg_build_ex": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
-                               C.c_float, C.c_uint32, C.c_uint32]),
+                               C.c_float, C.c_uint32, C.c_uint32, C.c_uint32, _vp]),
     "lqg_search": (C.c_int, [_vp, _vp, C.c_uint32, _vp]),
     "lqg_search_batch_device": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
                                           _vp, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp]),
@@ -70,6 +70,14 @@ class Tuning(C.Structure):
         ("heap_scap", C.c_uint32),
         ("replay_warps", C.c_uint32),
         ("replay_all", C.c_uint32),
+    ]
+
+
+class BuildReport(C.Structure):
+    _fields_ = [
+        ("prune_ms", C.c_double),
+        ("build_ms", C.c_double),
+        ("rechecks", C.c_uint64),
     ]
 
 

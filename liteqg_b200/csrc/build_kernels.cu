@@ -20,6 +20,7 @@
 // one CTA accumulates in registers over 128-dimension tiles staged in shared
 // memory.
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 #include <math_constants.h>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -194,6 +195,97 @@ __global__ void random_fill_kernel(uint32_t* __restrict__ out, const uint32_t* _
     __syncwarp();
 }
 
+// ---- candidate-to-candidate distances on the tensor cores (tcgen05) -------
+//
+// The prune's P x P matrix of squared distances among a node's candidates
+// (P <= 96) as one BF16 Gram matrix per 128-dimension chunk, accumulated in
+// FP32 in tensor memory: rows are the candidates minus the node's vector
+// (so norms are on the scale of the distances), rounded to BF16 and staged in
+// shared memory in the canonical K-major layout without swizzle (8-row x
+// 16-byte core matrices; the 16 core matrices of a row group's 128 dimensions
+// are 128 bytes apart (LBO), row groups 2048 bytes apart (SBO)). One thread
+// issues tcgen05.mma.cta_group::1.kind::f16 with M = 128 (rows past P are
+// zero), N = 96, K = 16 per instruction; the result is read back with
+// tcgen05.ld (warp w owns tensor-memory lanes 32w..32w+31) and
+// d~(i, j) = n~i + n~j - 2 G(i, j) with n~ the norms of the rounded rows.
+namespace tc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor (sm_100): start address, leading and
+// stride byte offsets (all >> 4), version 1, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor, kind::f16: BF16 A and B (K-major), FP32 D.
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(uint32_t m, uint32_t n) {
+    return (1u << 4)            // D format F32
+           | (1u << 7)          // A format BF16
+           | (1u << 10)         // B format BF16
+           | ((n >> 3) << 17)   // N / 8
+           | ((m >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n"
+        :
+        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u),
+          "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void commit(uint64_t* mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(mbar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+
+// Bounded wait for the mbarrier phase with this parity; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+    const uint32_t a = smem_u32(mbar);
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+}  // namespace tc
+
 // ---- candidate pruning ---------------------------------------------------
 
 // One CTA (kPruneThreads) per node.
@@ -227,32 +319,39 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     }
     __syncthreads();
 
-    // 1. gather (duplicates removed below after sorting by id). Entries are
-    // id << 1 | from_path (ids < 2^31).
-    auto add = [&](uint32_t v, uint32_t from_path) {
-        if (v == (uint32_t)node || v >= a.n) return;
-        const uint32_t s = atomicAdd(&s_cnt, 1u);
-        if (s < kCandMax) s_ids[s] = (v << 1) | from_path;
+    // 1. gather into fixed slots, source after source, up to kCandMax (so the
+    // candidate set does not depend on thread timing); duplicates removed
+    // below after sorting by id. Entries are id << 1 | from_path (ids < 2^31);
+    // the node itself and out-of-range ids become empty slots.
+    auto put = [&](uint32_t slot, uint32_t v, uint32_t from_path) {
+        s_ids[slot] = (v == (uint32_t)node || v >= a.n) ? 0xFFFFFFFFu : ((v << 1) | from_path);
     };
+    uint32_t off = 0;
     if (a.pool) {
         const uint32_t* p = a.pool + (node - a.node0) * a.pool_stride;
-        for (uint32_t j = tid; j < a.pool_take; j += kPruneThreads) add(p[j], 0u);
+        const uint32_t c = min(a.pool_take, (uint32_t)kCandMax - off);
+        for (uint32_t j = tid; j < c; j += kPruneThreads) put(off + j, p[j], 0u);
+        off += c;
     }
     if (a.path) {
         const uint32_t* p = a.path + (node - a.node0) * a.path_stride;
-        for (uint32_t j = tid; j < a.path_take; j += kPruneThreads) add(p[j], 1u);
+        const uint32_t c = min(a.path_take, (uint32_t)kCandMax - off);
+        for (uint32_t j = tid; j < c; j += kPruneThreads) put(off + j, p[j], 1u);
+        off += c;
     }
     if (a.nb) {
-        const uint32_t c = a.nb_cnt ? min(a.nb_cnt[node], a.deg) : a.deg;
-        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.nb[node * a.deg + j], 0u);
+        const uint32_t c = min(a.nb_cnt ? min(a.nb_cnt[node], a.deg) : a.deg, (uint32_t)kCandMax - off);
+        for (uint32_t j = tid; j < c; j += kPruneThreads) put(off + j, a.nb[node * a.deg + j], 0u);
+        off += c;
     }
     if (a.rev) {
         const uint32_t s0 = a.rev_start[node], s1 = a.rev_end[node];
-        const uint32_t c = min(s1 - s0, a.rev_cap);
-        for (uint32_t j = tid; j < c; j += kPruneThreads) add(a.rev[s0 + j], 0u);
+        const uint32_t c = min(min(s1 - s0, a.rev_cap), (uint32_t)kCandMax - off);
+        for (uint32_t j = tid; j < c; j += kPruneThreads) put(off + j, a.rev[s0 + j], 0u);
+        off += c;
     }
     __syncthreads();
-    const uint32_t cnt = min(s_cnt, (uint32_t)kCandMax);
+    const uint32_t cnt = off;
 
     // 2. exact distances node -> candidate (ids first sorted to drop dups)
     // bitonic sort by id to find duplicates
@@ -334,58 +433,157 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         }
     }
 
-    // 4. pairwise distances among the first P candidates, tiled over dims.
-    // Thread t owns pairs p = t + kPruneThreads * s of the strict upper
-    // triangle in row-major order.
-    constexpr int kPairsPerThread = (kPruneMax * (kPruneMax - 1) / 2 + kPruneThreads - 1) / kPruneThreads;
-    float acc[kPairsPerThread];
-    uint32_t pab[kPairsPerThread];  // row | col << 16
-    const uint32_t npairs = P * (P - (P > 0 ? 1 : 0)) / 2;
+    // 4. pairwise distances among the first P candidates
+    __shared__ uint64_t s_mbar;
+    __shared__ uint32_t s_tmem;
+    __shared__ float s_norm[128];
+    __shared__ int s_exact;
+    if (tid == 0) s_exact = 0;
+    if (a.pair_tc) {
+        // BF16 Gram matrices on the tensor cores (see tc:: above)
+        __nv_bfloat16* op = reinterpret_cast<__nv_bfloat16*>(tile);  // 128 rows x 128 dims, 32 KB
+        if (tid < 32) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                         ::"r"(tc::smem_u32(&s_tmem)), "r"(128u));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
+        if (tid == 0) {
+            tc::mbar_init(&s_mbar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tmem = s_tmem;
+        const float* xn = a.x + node * dim;
+        const float* xr = a.x + (uint64_t)(s_ids[tid < P ? tid : 0] >> 1) * dim;
+        float nrm = 0.f;
+        bool ok = true, rounded = false;
+        uint32_t chunk = 0;
+        for (uint32_t d0 = 0; d0 < dim; d0 += kTileD, ++chunk) {
+            // row tid of this chunk: bf16(x_candidate - x_node), zero past P and dim
+#pragma unroll 2
+            for (uint32_t kc = 0; kc < kTileD / 8; ++kc) {
+                uint32_t wv[4];
 #pragma unroll
-    for (int s = 0; s < kPairsPerThread; ++s) {
-        acc[s] = 0.f;
-        const uint32_t p = tid + kPruneThreads * s;
-        // invert p -> (r, c), r < c, row-major over the upper triangle of P
-        uint32_t r = 0, c = 0;
-        if (p < npairs) {
-            uint32_t rem = p;
-            uint32_t rowlen = P - 1;
-            while (rem >= rowlen) {
-                rem -= rowlen;
-                ++r;
-                --rowlen;
+                for (int e = 0; e < 4; ++e) {
+                    const uint32_t d = d0 + kc * 8 + 2 * e;
+                    float f0 = 0.f, f1 = 0.f;
+                    if (tid < P && d < dim) f0 = __fsub_rn(xr[d], xn[d]);
+                    if (tid < P && d + 1 < dim) f1 = __fsub_rn(xr[d + 1], xn[d + 1]);
+                    const __nv_bfloat162 b = __floats2bfloat162_rn(f0, f1);
+                    const float r0 = __low2float(b), r1 = __high2float(b);
+                    rounded |= r0 != f0 || r1 != f1;
+                    nrm = __fmaf_rn(r0, r0, nrm);
+                    nrm = __fmaf_rn(r1, r1, nrm);
+                    wv[e] = *reinterpret_cast<const uint32_t*>(&b);
+                }
+                *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(op) + kc * 128 +
+                                          (tid >> 3) * 2048 + (tid & 7) * 16) =
+                    make_uint4(wv[0], wv[1], wv[2], wv[3]);
             }
-            c = r + 1 + rem;
-        }
-        pab[s] = r | (c << 16);
-    }
-    for (uint32_t d0 = 0; d0 < dim; d0 += kTileD) {
-        const uint32_t td = min((uint32_t)kTileD, dim - d0);
-        __syncthreads();
-        for (uint32_t e = tid; e < P * td; e += kPruneThreads) {
-            const uint32_t r = e / td, c = e % td;
-            tile[r * (kTileD + 1) + c] = a.x[(uint64_t)(s_ids[r] >> 1) * dim + d0 + c];
-        }
-        __syncthreads();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t base = tc::smem_u32(op);
+                constexpr uint32_t idesc = tc::idesc_bf16_f32(128, kPruneMax);
 #pragma unroll
+                for (uint32_t s = 0; s < kTileD / 16; ++s) {
+                    const uint64_t dsc = tc::smem_desc(base + s * 256, 128, 2048);
+                    tc::mma_bf16(tmem, dsc, dsc, idesc, (chunk > 0 || s > 0) ? 1u : 0u);
+                }
+                tc::commit(&s_mbar);
+            }
+            // the operand tile is rewritten next chunk: wait for these MMAs
+            if (!tc::mbar_wait(&s_mbar, chunk & 1u)) ok = false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        }
+        s_norm[tid] = nrm;
+        // every staged value exact in BF16 and every norm below 2^23: the
+        // Gram matrix (its partial sums are bounded by the norms) and the
+        // distances are exact, so no decision needs a re-check
+        const int exact = !__syncthreads_or(rounded || nrm >= 8388608.0f);
+        if (tid == 0) s_exact = exact;
+        __syncthreads();
+        // row tid of the Gram matrix -> squared distances to every column
+        const uint32_t w = tid >> 5;
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < (uint32_t)kPruneMax; c0 += 16) {
+            float g[16];
+            tc::ld16(tmem + ((32u * w) << 16) + c0, g);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (tid < P) {
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const uint32_t c = c0 + e;
+                    if (c < P && c > tid)
+                        pair[tid * kPruneMax + c] =
+                            fmaxf(0.f, __fsub_rn(__fadd_rn(nrm, s_norm[c]), 2.f * g[e]));
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid < 32) {
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u));
+        }
+        if (!ok && tid == 0 && a.err) atomicOr(a.err, 1u);
+    } else {
+        if (tid < 128) s_norm[tid] = 0.f;
+        // 4. pairwise distances among the first P candidates, tiled over dims.
+        // Thread t owns pairs p = t + kPruneThreads * s of the strict upper
+        // triangle in row-major order.
+        constexpr int kPairsPerThread = (kPruneMax * (kPruneMax - 1) / 2 + kPruneThreads - 1) / kPruneThreads;
+        float acc[kPairsPerThread];
+        uint32_t pab[kPairsPerThread];  // row | col << 16
+        const uint32_t npairs = P * (P - (P > 0 ? 1 : 0)) / 2;
+    #pragma unroll
+        for (int s = 0; s < kPairsPerThread; ++s) {
+            acc[s] = 0.f;
+            const uint32_t p = tid + kPruneThreads * s;
+            // invert p -> (r, c), r < c, row-major over the upper triangle of P
+            uint32_t r = 0, c = 0;
+            if (p < npairs) {
+                uint32_t rem = p;
+                uint32_t rowlen = P - 1;
+                while (rem >= rowlen) {
+                    rem -= rowlen;
+                    ++r;
+                    --rowlen;
+                }
+                c = r + 1 + rem;
+            }
+            pab[s] = r | (c << 16);
+        }
+        for (uint32_t d0 = 0; d0 < dim; d0 += kTileD) {
+            const uint32_t td = min((uint32_t)kTileD, dim - d0);
+            __syncthreads();
+            for (uint32_t e = tid; e < P * td; e += kPruneThreads) {
+                const uint32_t r = e / td, c = e % td;
+                tile[r * (kTileD + 1) + c] = a.x[(uint64_t)(s_ids[r] >> 1) * dim + d0 + c];
+            }
+            __syncthreads();
+    #pragma unroll
+            for (int s = 0; s < kPairsPerThread; ++s) {
+                const uint32_t p = tid + kPruneThreads * s;
+                if (p < npairs) {
+                    const float* ra = tile + (pab[s] & 0xFFFFu) * (kTileD + 1);
+                    const float* rb = tile + (pab[s] >> 16) * (kTileD + 1);
+                    float t = acc[s];
+                    for (uint32_t c = 0; c < td; ++c) {
+                        const float df = ra[c] - rb[c];
+                        t = fmaf(df, df, t);
+                    }
+                    acc[s] = t;
+                }
+            }
+        }
+    #pragma unroll
         for (int s = 0; s < kPairsPerThread; ++s) {
             const uint32_t p = tid + kPruneThreads * s;
-            if (p < npairs) {
-                const float* ra = tile + (pab[s] & 0xFFFFu) * (kTileD + 1);
-                const float* rb = tile + (pab[s] >> 16) * (kTileD + 1);
-                float t = acc[s];
-                for (uint32_t c = 0; c < td; ++c) {
-                    const float df = ra[c] - rb[c];
-                    t = fmaf(df, df, t);
-                }
-                acc[s] = t;
-            }
+            if (p < npairs) pair[(pab[s] & 0xFFFFu) * kPruneMax + (pab[s] >> 16)] = acc[s];
         }
-    }
-#pragma unroll
-    for (int s = 0; s < kPairsPerThread; ++s) {
-        const uint32_t p = tid + kPruneThreads * s;
-        if (p < npairs) pair[(pab[s] & 0xFFFFu) * kPruneMax + (pab[s] >> 16)] = acc[s];
     }
     for (uint32_t i = tid; i < kPruneMax; i += kPruneThreads) {
         s_state[i] = 0;
@@ -413,8 +611,30 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         ++kept_n;
         if (!is_far) ++kept_near;
         if (tid == 0) s_keep[j] = 1;
-        for (uint32_t i = j + 1 + tid; i < P; i += kPruneThreads)
-            if (s_state[i] == 0 && a.alpha2 * pair[j * kPruneMax + i] < s_d[i]) s_state[i] = 2;
+        for (uint32_t i = j + 1 + tid; i < P; i += kPruneThreads) {
+            if (s_state[i] != 0) continue;
+            float dji = pair[j * kPruneMax + i];
+            if (a.pair_tc && !s_exact) {
+                // the BF16 estimate decides unless it lies within its error
+                // bound of the threshold; then the FP32 value, in the same
+                // order as the CUDA-core path, decides
+                const float ni = s_norm[i], nj = s_norm[j];
+                const float err = 0.015625f * sqrtf(fmaxf(dji, 0.f)) * (sqrtf(ni) + sqrtf(nj)) +
+                                  2.5e-4f * (ni + nj);
+                if (fabsf(a.alpha2 * dji - s_d[i]) <= a.alpha2 * err) {
+                    const float* xj = a.x + (uint64_t)(s_ids[j] >> 1) * dim;
+                    const float* xi = a.x + (uint64_t)(s_ids[i] >> 1) * dim;
+                    float t = 0.f;
+                    for (uint32_t d = 0; d < dim; ++d) {
+                        const float df = xj[d] - xi[d];
+                        t = fmaf(df, df, t);
+                    }
+                    dji = t;
+                    if (a.rechecks) atomicAdd(a.rechecks, 1ull);
+                }
+            }
+            if (a.alpha2 * dji < s_d[i]) s_state[i] = 2;
+        }
         __syncthreads();
     }
     __syncthreads();

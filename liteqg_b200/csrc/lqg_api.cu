@@ -778,15 +778,17 @@ lqg_status lqg_device_arrays(const lqg_index* ix, const uint32_t** nbrs, const u
 //              with its pruned candidates and, if still short, random ids.
 lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build, uint32_t num_iter,
                      uint64_t seed, uint32_t random_edges) {
-    return lqg_build_ex(ix, data, ef_build, num_iter, seed, random_edges, 1.0f, 0, 0);
+    return lqg_build_ex(ix, data, ef_build, num_iter, seed, random_edges, 1.0f, 0, 0, 1, nullptr);
 }
 
 lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uint32_t num_iter,
                         uint64_t seed, uint32_t random_edges, float alpha, uint32_t path_take,
-                        uint32_t far_budget) {
+                        uint32_t far_budget, uint32_t pair_kernel, lqg_build_report* report) {
     if (!ix || !data) return fail(LQG_ERR_ARG, "null argument");
+    if (pair_kernel > 1) return fail(LQG_ERR_ARG, "pair_kernel must be 0 or 1");
+    if (report) *report = lqg_build_report{};
     if (!(alpha >= 1.0f && alpha <= 4.0f)) return fail(LQG_ERR_ARG, "alpha must be in [1, 4]");
-    if (path_take > 256) return fail(LQG_ERR_ARG, "path_take must be <= 256");
+    if (path_take > 128) return fail(LQG_ERR_ARG, "path_take must be <= 128");
     if (far_budget + random_edges >= ix->deg)
         return fail(LQG_ERR_ARG, "far_budget + random_edges must be below degree_bound");
     const float alpha2 = alpha * alpha;
@@ -821,8 +823,11 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
     uint32_t *d_kept = nullptr, *d_kept_cnt = nullptr, *d_rest = nullptr, *d_rest_cnt = nullptr;
     uint32_t *d_new = nullptr, *d_new_cnt = nullptr;
     lqg::ReverseWork rw{};
-    uint32_t *d_pool = nullptr, *d_k1 = nullptr, *d_path = nullptr;
+    uint32_t *d_pool = nullptr, *d_k1 = nullptr, *d_path = nullptr, *d_perr = nullptr;
+    unsigned long long* d_rechk = nullptr;
     float* d_pool_d = nullptr;
+    cudaEvent_t evb[4] = {nullptr, nullptr, nullptr, nullptr};
+    double prune_ms = 0.0;
     // the build searches run the fast kernel with ties resolved by insertion order
     const lqg_tuning saved_tune = ix->tune;
     ix->tune.mode = 1;
@@ -832,7 +837,8 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
         dfree(d_rest_cnt); dfree(d_new); dfree(d_new_cnt);
         dfree(rw.keys_in); dfree(rw.vals_in); dfree(rw.keys_out); dfree(rw.vals_out);
         dfree(rw.start); dfree(rw.end); if (rw.temp) cudaFree(rw.temp); rw.temp = nullptr;
-        dfree(d_pool); dfree(d_k1); dfree(d_pool_d); dfree(d_path);
+        dfree(d_pool); dfree(d_k1); dfree(d_pool_d); dfree(d_path); dfree(d_perr); dfree(d_rechk);
+        for (auto& e : evb) if (e) { cudaEventDestroy(e); e = nullptr; }
         ix->tune = saved_tune;
     };
     auto alloc = [&](auto*& p, size_t bytes) {
@@ -857,12 +863,19 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
               alloc(d_new, n * deg * 4) && alloc(d_new_cnt, n * 4) &&
               alloc(d_pool, chunk * ef_build * 4) && alloc(d_pool_d, chunk * ef_build * 4) &&
               alloc(d_k1, chunk * 4) && (ix->cstride == dim || alloc(d_c, n * dim)) &&
-              (path_take == 0 || alloc(d_path, chunk * path_take * 4));
+              (path_take == 0 || alloc(d_path, chunk * path_take * 4)) && alloc(d_perr, 4) &&
+              alloc(d_rechk, 8);
     if (!ok) {
         cleanup();
         return fail(LQG_ERR_NOMEM, "device allocation for the build failed");
     }
     cudaStream_t st = nullptr;
+    for (auto& e : evb)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            cleanup();
+            return fail(LQG_ERR_CUDA, "event creation failed");
+        }
     auto check_cuda = [&](cudaError_t e, const char* what) -> lqg_status {
         if (e == cudaSuccess) return LQG_OK;
         cleanup();
@@ -872,6 +885,20 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
 #define LQG_BCUDA(call, what) \
     if ((s = check_cuda((call), what)) != LQG_OK) return s
     LQG_BCUDA(cudaMemcpy(d_x, data, n * dim * 4, cudaMemcpyHostToDevice), "copy data");
+    LQG_BCUDA(cudaMemset(d_perr, 0, 4), "build flags");
+    LQG_BCUDA(cudaMemset(d_rechk, 0, 8), "build flags");
+    LQG_BCUDA(cudaEventRecord(evb[0], st), "event");
+    // prune launches are timed between evb[2] and evb[3]
+    auto timed_prune = [&](const lqg::PruneArgs& pa, uint64_t nodes) -> cudaError_t {
+        cudaError_t e = cudaEventRecord(evb[2], st);
+        if (e == cudaSuccess) e = lqg::launch_prune(pa, nodes, st);
+        if (e == cudaSuccess) e = cudaEventRecord(evb[3], st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(evb[3]);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, evb[2], evb[3]);
+        prune_ms += ms;
+        return e;
+    };
     uint8_t* codes_out = ix->cstride == dim ? ix->d_codes : d_c;
     LQG_BCUDA(lqg::launch_sq8_encode(d_x, n, dim, ix->d_params, codes_out, (float*)d_work, st),
               "sq8 encode");
@@ -908,7 +935,9 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
             a.node0 = c0;
             a.pool = d_pool;
             a.pool_stride = ef_build;
-            a.pool_take = std::min<uint32_t>(ef_build, lqg::kCandMax - deg);
+            // candidates: pool, then search path, then the current list
+            a.pool_take = std::min<uint32_t>(
+                ef_build, std::max<int>(64, (int)lqg::kCandMax - (int)deg - (int)path_take));
             a.nb = ix->d_nbrs;
             a.out = d_kept;
             a.out_cnt = d_kept_cnt;
@@ -921,7 +950,10 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
             a.path_take = path_take;
             a.far_take = std::min<uint32_t>(path_take, 32);
             a.far_budget = far_budget;
-            LQG_BCUDA(lqg::launch_prune(a, m, st), "prune");
+            a.pair_tc = (int)pair_kernel;
+            a.err = d_perr;
+            a.rechecks = d_rechk;
+            LQG_BCUDA(timed_prune(a, m), "prune");
         }
         LQG_BCUDA(lqg::launch_reverse(d_kept, d_kept_cnt, n, deg, rw, st), "reverse edges");
         lqg::PruneArgs b{};
@@ -945,7 +977,10 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
         b.rest_fill = d_rest;
         b.rest_fill_cnt = d_rest_cnt;
         b.rest_stride = rest_stride;
-        LQG_BCUDA(lqg::launch_prune(b, n, st), "merge reverse edges");
+        b.pair_tc = (int)pair_kernel;
+        b.err = d_perr;
+        b.rechecks = d_rechk;
+        LQG_BCUDA(timed_prune(b, n), "merge reverse edges");
         LQG_BCUDA(lqg::launch_random_fill(d_new, d_new_cnt, n, deg, seed + 1 + it, st), "fill");
         LQG_BCUDA(cudaMemcpy(ix->d_nbrs, d_new, n * deg * 4, cudaMemcpyDeviceToDevice), "graph");
     }
@@ -953,7 +988,24 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
     LQG_BCUDA(cudaMemcpy2D(ix->codes.data(), dim, ix->d_codes, ix->cstride, dim, n,
                            cudaMemcpyDeviceToHost), "codes");
     LQG_BCUDA(cudaMemcpy(ix->params.data(), ix->d_params, dim * 8, cudaMemcpyDeviceToHost), "params");
+    LQG_BCUDA(cudaEventRecord(evb[1], st), "event");
+    LQG_BCUDA(cudaEventSynchronize(evb[1]), "event");
+    uint32_t perr = 0;
+    unsigned long long rechk = 0;
+    LQG_BCUDA(cudaMemcpy(&perr, d_perr, 4, cudaMemcpyDeviceToHost), "build flags");
+    LQG_BCUDA(cudaMemcpy(&rechk, d_rechk, 8, cudaMemcpyDeviceToHost), "build flags");
+    if (report) {
+        float bms = 0.f;
+        cudaEventElapsedTime(&bms, evb[0], evb[1]);
+        report->build_ms = bms;
+        report->prune_ms = prune_ms;
+        report->rechecks = rechk;
+    }
 #undef LQG_BCUDA
+    if (perr) {
+        cleanup();
+        return fail(LQG_ERR_CUDA, "build: a tensor-core wait in the prune timed out");
+    }
     cleanup();
     return validate_content(ix);
 }

@@ -46,6 +46,12 @@ struct PruneArgs {
     // slots of a list that only candidates farther than 4x the nearest
     // candidate's squared distance may take (long links)
     uint32_t far_budget;
+    // candidate-to-candidate distances: 0 FP32 on the CUDA cores; 1 BF16 Gram
+    // matrices on the tensor cores (tcgen05) with FP32 re-checks of the
+    // decisions near their threshold
+    int pair_tc;
+    uint32_t* err;                   // bit 0: a tensor-core wait timed out
+    unsigned long long* rechecks;    // FP32 re-checks made (or null)
 };
 
 cudaError_t launch_sq8_encode(const float* x, uint64_t n, uint32_t dim, float* params,

@@ -26,7 +26,7 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
-from ._capi import LQG_NO_ID, LqgError, Tuning, check, lib
+from ._capi import LQG_NO_ID, BuildReport, LqgError, Tuning, check, lib
 
 UINT_MAX = 0xFFFFFFFF
 
@@ -87,14 +87,18 @@ class Index:
 
     def build_index(self, data, EF: int, num_iter: int = 3, num_thread: int = UINT_MAX,
                     seed: int = 0, random_edges: int | None = None,
-                    alpha: float = 1.0, path_take: int = 0, far_budget: int = 0) -> None:
+                    alpha: float = 1.0, path_take: int = 0, far_budget: int = 0,
+                    pair_kernel: int = 1) -> dict:
         """Builds on the GPU (``num_thread`` is accepted and unused).
 
         ``random_edges`` slots of each neighbour list hold seeded random
         long-range links (default ``degree_bound // 8``); ``alpha`` >= 1 is
         the prune's occlusion factor (1 = the reference's heuristic);
         ``path_take`` search-path nodes join each node's candidates and
-        ``far_budget`` slots are held for long links (see lqg_build_ex)."""
+        ``far_budget`` slots are held for long links; ``pair_kernel`` 1 runs
+        the prune's distance matrices as BF16 tcgen05 GEMMs with FP32
+        re-checks, 0 in FP32 on CUDA cores (same graph; see lqg_build_ex).
+        Returns the build report (prune/build ms, FP32 re-checks)."""
         items = _as_f32(data)
         if items.ndim == 1:
             items = items.reshape(1, -1)
@@ -105,8 +109,11 @@ class Index:
         if num_iter <= 1:
             raise ValueError("The number of iter for building qg should >= 3")
         re = self.degree_bound // 8 if random_edges is None else int(random_edges)
+        rep = BuildReport()
         check(lib().lqg_build_ex(self.handle, _p(items), int(EF), int(num_iter), int(seed), re,
-                                 float(alpha), int(path_take), int(far_budget)))
+                                 float(alpha), int(path_take), int(far_budget), int(pair_kernel),
+                                 C.byref(rep)))
+        return {f: getattr(rep, f) for f, _ in BuildReport._fields_}
 
     def search(self, query, k: int, ef=None, return_pool: bool = False,
                return_stats: bool = False):

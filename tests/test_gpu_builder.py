@@ -103,3 +103,30 @@ def test_build_search_path_links_reach_every_cluster():
             assert np.array_equal(again.get_arrays()[2], nb)
     assert rec["path"] >= rec["random"], rec
     assert rec["path"] >= 0.9, rec
+
+
+@pytest.mark.parametrize("kind", ["uniform", "int_mixture", "gauss_mixture"])
+def test_tensor_core_prune_builds_the_fp32_graph(kind):
+    """pair_kernel 1 (BF16 tcgen05 Gram matrices, FP32 re-check of decisions
+    near their threshold) builds exactly the graph of pair_kernel 0 (FP32 on
+    CUDA cores): no pruned edge differs."""
+    import liteqg_b200
+
+    rng = np.random.default_rng(17)
+    n, dim, deg = 12000, 128, 32
+    if kind == "uniform":
+        x = rng.random((n, dim), dtype=np.float32)
+    elif kind == "int_mixture":
+        c = rng.uniform(0, 255, (48, dim))
+        x = np.clip(np.rint(c[rng.integers(0, 48, n)] + rng.normal(0, 20, (n, dim))), 0, 255).astype(np.float32)
+    else:
+        c = rng.normal(0, 1, (48, dim))
+        x = (c[rng.integers(0, 48, n)] + rng.normal(0, 0.3, (n, dim))).astype(np.float32)
+    graphs, reps = [], []
+    for pk in (0, 1):
+        ix = liteqg_b200.Index("QG", "L2", n, dim, deg)
+        reps.append(ix.build_index(x, 100, num_iter=3, random_edges=4, path_take=32, far_budget=4,
+                                   pair_kernel=pk))
+        graphs.append(ix.get_arrays()[2])
+    assert np.array_equal(graphs[0], graphs[1]), int((graphs[0] != graphs[1]).any(1).sum())
+    assert reps[0]["rechecks"] == 0 and reps[1]["prune_ms"] > 0
