@@ -230,14 +230,19 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per query of the dominant kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "heap_search_traffic.json")
+def profile_traffic(kernel, name, ef):
+    """DRAM bytes per query of `kernel` on workload `name` at this ef, from the
+    committed ncu summaries (None when no capture matches)."""
+    p = os.path.join(ROOT, "profiles", "search_traffic.json")
     try:
         with open(p) as f:
-            return json.load(f)
+            rows = json.load(f)
     except Exception:
         return None
+    for r in rows:
+        if r.get("kernel") == kernel and r.get("workload") == name and r.get("ef") == ef:
+            return float(r["dram_bytes_per_query"])
+    return None
 
 
 def cpu_reference_search(path, w, queries, k, ef, nthreads):
@@ -486,11 +491,9 @@ def gpu_arm(args, w, name, rank, world, device):
     else:
         cpu = None
 
-    traffic = profile_traffic()
-    traffic_launch = None
-    if (traffic and traffic.get("workload") == name and traffic.get("ef") == chosen
-            and mode == 2):
-        traffic_launch = traffic["dram_bytes_per_query"] * nq
+    kernel = {2: "heap_search_kernel", 4: "split_search_kernel", 5: "batch_search_kernel"}.get(mode)
+    per_query = profile_traffic(kernel, name, chosen) if kernel else None
+    traffic_launch = per_query * nq if per_query is not None else None
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": K,
         "warmup": max(3, args.warmup), "ms_per_step": statistics.mean(step_ms),
@@ -511,12 +514,14 @@ def gpu_arm(args, w, name, rank, world, device):
                      "kernel_ms": statistics.mean(kern_ms),
                      "kernel": {1: "fast_search_kernel + heap_search_kernel (tied queries)",
                                 2: "heap_search_kernel",
-                                4: "split_search_kernel"}.get(mode, str(mode))},
+                                4: "split_search_kernel",
+                                5: "batch_search_kernel"}.get(mode, str(mode))},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": int(nq * dim * 4),
                 "d2h_bytes_per_step": int(nq * k * 4)},
         # kernels per batched step: fast + heap + exact (1), heap + exact (2),
-        # replay + result replay + exact (3), split + exact (4); the L2 flush is torch's
-        "gpu_launches": {1: 3, 2: 2, 3: 3, 4: 2}.get(mode, 3) * K,
+        # replay + result replay + exact (3), split or batch + exact (4, 5); the
+        # L2 flush is torch's
+        "gpu_launches": {1: 3, 2: 2, 3: 3, 4: 2, 5: 2}.get(mode, 3) * K,
         "clocks": clk.summary(),
         "p50_ms": statistics.median(step_ms), "p99_ms": float(np.percentile(step_ms, 99)),
         **extra,
@@ -695,6 +700,27 @@ def serving_arm(args, w, name, device):
     print(json.dumps(line), flush=True)
 
 
+def build_only(w, name, device):
+    """One GPU build of the workload's index inside an NVTX range 'lqg_build'
+    (the range a profiler filters on); prints the build report as JSON."""
+    import torch
+
+    import liteqg_b200
+
+    base = gen_data(w, "base")
+    ix = liteqg_b200.Index("QG", "L2", w["n"], w["dim"], w["deg"], device=device)
+    torch.cuda.nvtx.range_push("lqg_build")
+    t = time.perf_counter()
+    rep = ix.build_index(base, w["efb"], num_iter=w["iters"], random_edges=w["random_edges"],
+                         path_take=w["path_take"], far_budget=w["far_budget"])
+    wall = time.perf_counter() - t
+    torch.cuda.nvtx.range_pop()
+    ix.close()
+    print(json.dumps({"workload": name, "n": w["n"], "dim": w["dim"], "deg": w["deg"],
+                      "ef_build": w["efb"], "iters": w["iters"], "wall_s": wall,
+                      "report": rep}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -704,8 +730,13 @@ def main():
     ap.add_argument("--workload", default="batched-1m128", choices=sorted(WORKLOADS))
     ap.add_argument("--profile", type=int, default=0,
                     help="run N batched steps inside an NVTX range 'lqg_profile' and exit")
+    ap.add_argument("--build-only", action="store_true",
+                    help="build the workload's index (no cache), print the build report, exit")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
+    if args.build_only:
+        build_only(w, args.workload, int(os.environ.get("LOCAL_RANK", "0")))
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

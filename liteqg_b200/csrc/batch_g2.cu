@@ -1,0 +1,7 @@
+// Batched-acceptance search kernel instances with 2 lanes per candidate.
+#include "batch_kernel.cuh"
+
+namespace lqg {
+template cudaError_t batch_dispatch<2>(const SearchArgs&, const ReplayArgs&, int, int, int,
+                                       cudaStream_t, int*);
+}  // namespace lqg

@@ -66,37 +66,56 @@ __device__ __forceinline__ void warp_push(HeapView h, uint32_t& n, uint2 v, int 
     ++n;
 }
 
-// pop_heap + pop_back.
+// pop_heap + pop_back. The hole walk of __adjust_heap goes five levels per
+// round: lane i (< 31) takes the i-th node, in breadth-first order, of the
+// five-level subtree under the hole, loads its two children and decides
+// which one the walk would take from it (left only if comp(right, left)) and
+// whether the walk continues there (node < (len - 1) / 2). One ballot per
+// bit gives the path; each lane on it moves its chosen child up into its
+// node. All loads of a round precede its stores and no path node is read
+// after it is written, so the moves are the sequential walk's.
 __device__ __forceinline__ void warp_pop(HeapView h, uint32_t& n, int lane) {
     const uint32_t size = n;
     if (size > 1) {
+        const uint32_t len = size - 1;
+        const uint2 v = h.get(len);
+        const uint32_t lim = (len - 1) / 2;
         uint32_t hole = 0;
-        uint2 v = make_uint2(0, 0);
-        if (lane == 0) {
-            const uint32_t len = size - 1;
-            v = h.get(len);
-            uint32_t second = 0;
-            while (second < (len - 1) / 2) {
-                second = 2 * (second + 1);
-                const uint2 r = h.get(second), l = h.get(second - 1);
-                if (hless(r, l)) {
-                    second--;
-                    h.set(hole, l);
-                } else {
-                    h.set(hole, r);
-                }
-                hole = second;
+        // BFS index i: depth k = floor(log2(i + 1)), offset i + 1 - 2^k
+        const uint32_t k = 31u - __clz((uint32_t)lane + 1u);
+        const uint32_t off = (uint32_t)lane + 1u - (1u << k);
+        while (hole < lim) {
+            const uint32_t node = ((hole + 1u) << k) - 1u + off;
+            const bool cont = lane < 31 && node < lim;
+            uint2 ch = make_uint2(0, 0);
+            bool left = false;
+            if (cont) {
+                const uint2 r = h.get(2 * node + 2), l = h.get(2 * node + 1);
+                left = hless(r, l);
+                ch = left ? l : r;
             }
-            if ((len & 1u) == 0 && second == (len - 2) / 2) {
-                second = 2 * (second + 1);
-                h.set(hole, h.get(second - 1));
-                hole = second - 1;
+            const unsigned mc = __ballot_sync(kFull, cont);
+            const unsigned ml = __ballot_sync(kFull, left);
+            uint32_t i = 0, path = 0;
+            int steps = 0;
+            while (steps < 5 && ((mc >> i) & 1u)) {
+                path |= 1u << i;
+                i = 2 * i + (((ml >> i) & 1u) ? 1u : 2u);
+                ++steps;
             }
+            if ((path >> lane) & 1u) h.set(node, ch);
+            __syncwarp();
+            // the hole moves to BFS index i (depth `steps`) of this subtree
+            hole = ((hole + 1u) << steps) - 1u + (i + 1u - (1u << steps));
+            if (steps < 5) break;
         }
-        __syncwarp();
-        hole = __shfl_sync(kFull, hole, 0);
-        v.x = __shfl_sync(kFull, v.x, 0);
-        v.y = __shfl_sync(kFull, v.y, 0);
+        if ((len & 1u) == 0 && hole == (len - 2) / 2) {
+            const uint2 c = h.get(2 * hole + 1);
+            __syncwarp();
+            if (lane == 0) h.set(hole, c);
+            __syncwarp();
+            hole = 2 * hole + 1;
+        }
         warp_sift_up(h, hole, v, lane);
     }
     n = size - 1;

@@ -203,11 +203,13 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     const bool heap_all = t.mode == 2;
     cudaError_t e;
 
-    if (t.mode == 3 || t.mode == 4) {
-        // replay (3) or split (4) kernel over every query, then the result
-        // replay pass, in chunks whose result logs fit 1 GiB; spilled queries
-        // go to the exact kernel
-        const bool split = t.mode == 4;
+    if (t.mode == 3 || t.mode == 4 || t.mode == 5) {
+        // replay (3), split (4) or batch (5) kernel over every query, then the
+        // result replay pass where the search warps do not replay in place, in
+        // chunks whose result logs fit 1 GiB; spilled queries go to the exact
+        // kernel
+        const bool batch = t.mode == 5;
+        const bool split = t.mode == 4 || batch;
         const int RE = lqg::replay_pool_regs(b.ef0);
         if (RE == 0) return fail(LQG_ERR_ARG, "ef too large for the replay kernels");
         lqg::ReplayArgs ra{};
@@ -218,6 +220,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         ra.nspill = w.d_ctl + kCtlSpilled;
         ra.rlog_cap = std::max(1024u, 16u * b.ef0);
         ra.replay_all = t.replay_all;
+        ra.acap = 32u * (uint32_t)RE;
         const int64_t chunk = std::min<int64_t>(
             b.m, std::max<int64_t>(1024, (int64_t(1) << 30) / ((int64_t)ra.rlog_cap * 16)));
         if ((s = grow(w.d_rlog, w.cap_rlog, (size_t)chunk * ra.rlog_cap)) != LQG_OK) return s;
@@ -226,7 +229,11 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         ra.rlen = w.d_rlen;
         // split kernel blocks hold at most 5 warps (its 96-register budget)
         int sw = plain ? 1 : (int)(split ? std::min(t.heap_warps, 5u) : t.replay_warps);
-        if (split) {
+        if (batch) {
+            while (sw > 1 &&
+                   lqg::batch_smem_bytes(ix->dim, t.visited_bits, ra.scap, ra.acap, sw) > 227 * 1024)
+                --sw;
+        } else if (split) {
             while (sw > 1 && lqg::split_smem_bytes(ix->dim, t.visited_bits, ra.scap, sw) > 227 * 1024)
                 --sw;
         } else {
@@ -238,6 +245,8 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         h.qhead = w.d_ctl + kCtlHeapHead;
         h.vbits = t.visited_bits;
         auto launch = [&](const SearchArgs& c, int blocks, int* occ) {
+            if (batch)
+                return lqg::launch_batch(c, ra, (int)t.lanes_per_cand, degw, sw, blocks, b.st, occ);
             return split ? lqg::launch_split(c, ra, RE, (int)t.lanes_per_cand, degw, sw, blocks, b.st, occ)
                          : lqg::launch_replay(c, ra, RE, (int)t.lanes_per_cand, degw, blocks, b.st, occ);
         };
@@ -284,8 +293,10 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             const int cb = (int)std::min<int64_t>(rb, (mc + sw - 1) / sw);
             e = launch(c, cb, nullptr);
             if (e != cudaSuccess) return cuda_fail(e, "search launch");
-            if (!split || ra.replay_all ||
-                !lqg::split_replays_in_place_host(t.visited_bits, ra.scap, ra.rcap)) {
+            const bool in_place =
+                batch ? lqg::batch_replays_in_place_host(t.visited_bits, ra.scap, ra.acap, ra.rcap)
+                      : lqg::split_replays_in_place_host(t.visited_bits, ra.scap, ra.rcap);
+            if (!split || ra.replay_all || !in_place) {
                 e = lqg::launch_rp_replay(c, ra, b.st);
                 if (e != cudaSuccess) return cuda_fail(e, "result replay launch");
             }
@@ -705,7 +716,7 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         n.blocks_per_sm = t->blocks_per_sm;
     }
     if (t->mode) {
-        if (t->mode > 4) return fail(LQG_ERR_ARG, "mode must be 1, 2, 3 or 4");
+        if (t->mode > 5) return fail(LQG_ERR_ARG, "mode must be 1, 2, 3, 4 or 5");
         n.mode = t->mode;
     }
     if (t->heap_warps) {
@@ -726,6 +737,10 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         return fail(LQG_ERR_ARG, "replay kernel tuning needs more than 227 KB of shared memory");
     if (n.mode == 4 && lqg::split_smem_bytes(ix->dim, n.visited_bits, n.heap_scap, 1) > 227 * 1024)
         return fail(LQG_ERR_ARG, "split kernel tuning needs more than 227 KB of shared memory");
+    if (n.mode == 5 && lqg::batch_smem_bytes(ix->dim, n.visited_bits, n.heap_scap,
+                                             32u * (uint32_t)lqg::replay_pool_regs(kMaxEf), 1) >
+                           227 * 1024)
+        return fail(LQG_ERR_ARG, "batch kernel tuning needs more than 227 KB of shared memory");
     if (n.mode <= 2 &&
         lqg::heap_smem_bytes(ix->dim, n.visited_bits, kMaxEf + 2, n.heap_scap, (int)n.heap_warps) >
         227 * 1024)

@@ -58,8 +58,9 @@ struct ReplayArgs {
     uint32_t* rlen;      // [m] accepted nodes logged, 0xFFFFFFFF if the search failed
     uint32_t rcap;       // result-heap slots (>= ef + 1) of the replay pass
     uint32_t efcap;      // largest ef: min(sorted-pool slots - 32, rcap - 1)
-    uint32_t replay_all; // split kernel: replay every query's result heap (else only
-                         // those whose output the heap layout decides)
+    uint32_t replay_all; // split/batch kernels: replay every query's result heap (else
+                         // only those whose output the heap layout decides)
+    uint32_t acap;       // batch kernel: sorted-pool slots (>= efcap + 32)
 };
 constexpr uint32_t kRlenDone = 0xFFFFFFFEu;  // rlen: output already written
 constexpr uint32_t kReplayLogN = 128;  // search-heap log ring entries (8 bytes) per search warp
@@ -81,6 +82,12 @@ size_t split_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t scap, int warps);
 bool split_replays_in_place_host(uint32_t vbits, uint32_t scap, uint32_t rcap);
 cudaError_t launch_split(const SearchArgs& a, const ReplayArgs& ra, int E, int G, int degw,
                          int warps, int blocks, cudaStream_t st, int* occ);
+// Batched-acceptance kernel (batch_kernel.cuh): exact search heap per warp,
+// sorted pool in shared memory, each expansion's candidates decided at once.
+size_t batch_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t scap, uint32_t acap, int warps);
+bool batch_replays_in_place_host(uint32_t vbits, uint32_t scap, uint32_t acap, uint32_t rcap);
+cudaError_t launch_batch(const SearchArgs& a, const ReplayArgs& ra, int G, int degw, int warps,
+                         int blocks, cudaStream_t st, int* occ);
 // Result-heap replay pass over a[0, m): one warp per query.
 cudaError_t launch_rp_replay(const SearchArgs& a, const ReplayArgs& ra, cudaStream_t st);
 

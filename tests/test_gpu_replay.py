@@ -1,10 +1,13 @@
-"""GPU parity of the replay (tuning mode 3) and split (mode 4) kernels through the C ABI.
+"""GPU parity of the replay (tuning mode 3), split (mode 4) and batch (mode 5)
+kernels through the C ABI.
 
 Mode 3: search warps run the sorted-pool form of the reference's loop and log
 every search-pool operation; a replay lane runs the reference's libstdc++
 search heap from the log, checks each step, and answers when equal distances
 make the heap layout decide. Mode 4: each search warp runs the exact search
-heap itself and keeps only a sorted array for the bound. In both, the result
+heap itself and keeps only a sorted array for the bound. Mode 5: as mode 4,
+with the sorted pool in shared memory and every expansion's candidates
+accepted or rejected at once from a rank count. In all, the result
 heap is replayed afterwards from a per-query log by one warp per query,
 which checks every acceptance and writes the output. Bar: ids, FP32 pools and
 pop counts bit-exact against the reference's golden outputs and the oracle;
@@ -29,7 +32,8 @@ def lqg():
 # (tuning mode, replay_all): the split kernel writes unambiguous outputs from
 # its sorted array; replay_all=1 sends every query through the checked result
 # replay pass instead, so both paths are covered.
-@pytest.fixture(params=[(3, 0), (4, 0), (4, 1)], ids=["replay", "split", "split-replay-all"])
+@pytest.fixture(params=[(3, 0), (4, 0), (4, 1), (5, 0), (5, 1)],
+                ids=["replay", "split", "split-replay-all", "batch", "batch-replay-all"])
 def mode(request):
     return request.param
 
