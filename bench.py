@@ -491,7 +491,8 @@ def gpu_arm(args, w, name, rank, world, device):
     else:
         cpu = None
 
-    kernel = {2: "heap_search_kernel", 4: "split_search_kernel", 5: "batch_search_kernel"}.get(mode)
+    kernel = {2: "heap_search_kernel", 4: "split_search_kernel", 5: "batch_search_kernel",
+              6: "batch_search_kernel (lazy search heap)"}.get(mode)
     per_query = profile_traffic(kernel, name, chosen) if kernel else None
     traffic_launch = per_query * nq if per_query is not None else None
     line = {
@@ -515,13 +516,14 @@ def gpu_arm(args, w, name, rank, world, device):
                      "kernel": {1: "fast_search_kernel + heap_search_kernel (tied queries)",
                                 2: "heap_search_kernel",
                                 4: "split_search_kernel",
-                                5: "batch_search_kernel"}.get(mode, str(mode))},
+                                5: "batch_search_kernel",
+                                6: "batch_search_kernel (lazy search heap)"}.get(mode, str(mode))},
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": int(nq * dim * 4),
                 "d2h_bytes_per_step": int(nq * k * 4)},
         # kernels per batched step: fast + heap + exact (1), heap + exact (2),
-        # replay + result replay + exact (3), split or batch + exact (4, 5); the
+        # replay + result replay + exact (3), split or batch + exact (4-6); the
         # L2 flush is torch's
-        "gpu_launches": {1: 3, 2: 2, 3: 3, 4: 2, 5: 2}.get(mode, 3) * K,
+        "gpu_launches": {1: 3, 2: 2, 3: 3, 4: 2, 5: 2, 6: 2}.get(mode, 3) * K,
         "clocks": clk.summary(),
         "p50_ms": statistics.median(step_ms), "p99_ms": float(np.percentile(step_ms, 99)),
         **extra,

@@ -217,15 +217,18 @@ LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
  *                   warp, result heap replayed afterwards from a log);
  *                   5: batch kernel for every query (as 4, with each
  *                   expansion's candidates decided at once against a
- *                   sorted pool in shared memory)
+ *                   sorted pool in shared memory); 6: batch kernel with
+ *                   the search heap built only when a pop meets equal
+ *                   smallest distances (until then the heap's top is the
+ *                   sorted pool's first unpopped entry)
  *   heap_warps      {1..8}: warps per block of the heap kernel, {1..5} of
- *                   the split and batch kernels
+ *                   the split and batch kernels (modes 4-6)
  *   heap_scap       [256, 16384]: search-pool slots per query in shared
  *                   memory (heap and replay kernels; larger pools spill to
  *                   global memory, then to the global-memory kernel)
  *   replay_warps    {1..15}: search warps per block of the replay kernel
  *                   (plus one replay warp)
- *   replay_all      modes 4, 5: 1 sends every query through the checked result
+ *   replay_all      modes 4-6: 1 sends every query through the checked result
  *                   replay pass (0, the default: only queries whose output
  *                   the heap layout decides); set on every call, not kept
  *                   when 0 is passed */

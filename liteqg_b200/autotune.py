@@ -1,7 +1,7 @@
 """Autotuner for the search kernels' launch shape and policy.
 
 Times a small grid of `lqg_tuning` settings (kernel mode: 1 fast + heap for
-tied queries, 2 heap, 4 split, 5 batch; lanes per candidate, visited-cache size, warps
+tied queries, 2 heap, 4 split, 5 batch, 6 batch with a lazy search heap; lanes per candidate, visited-cache size, warps
 per block, shared-memory search-pool slots) on a
 sample of the caller's queries with CUDA events, keeps the fastest, and caches
 the choice in a JSON file keyed on (N, D, degree, ef, k), so later runs on the
@@ -19,6 +19,12 @@ DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "liteqg_b200", "
 
 # (mode, lanes_per_cand, visited_bits, warps_per_block, heap_warps, heap_scap)
 CANDIDATES = [
+    (6, 2, 10, 8, 4, 256),
+    (6, 4, 10, 8, 4, 256),
+    (6, 2, 10, 8, 5, 256),
+    (6, 4, 10, 8, 5, 256),
+    (6, 2, 10, 8, 4, 512),
+    (6, 2, 9, 8, 5, 256),
     (5, 2, 10, 8, 4, 256),
     (5, 4, 10, 8, 4, 256),
     (5, 2, 10, 8, 4, 512),

@@ -69,6 +69,42 @@ __host__ __device__ inline bool batch_replays_in_place(uint32_t vbits, uint32_t 
            8 * (size_t)rcap;
 }
 
+constexpr uint32_t kPopped = 0x80000000u;  // sorted-pool id flag (ids are < 2^31)
+
+// Rebuilds the search heap of a query that ran without it (lazy mode): the
+// reference's pushes (every accepted node in order, read from the result log)
+// and pops (each after the logged number of pushes) replayed on an empty
+// heap. Every replayed pop must return the node the lazy search popped there.
+// Returns false, with the heap unusable, when one does not or the heap would
+// outgrow its slots.
+__device__ __forceinline__ bool rebuild_search_heap(const heapops::HeapView sp, uint32_t& sn,
+                                                    uint32_t sp_max, const uint4* rlog,
+                                                    const uint2* plog, uint32_t acc_n,
+                                                    uint32_t pops, int lane) {
+    using namespace heapops;
+    sn = 0;
+    uint32_t i = 0;
+    for (uint32_t j = 0; j <= pops; ++j) {
+        const uint2 pj = j < pops ? plog[j] : make_uint2(acc_n, kNoId);
+        while (i < pj.x) {
+            const uint32_t cnt = min(32u, pj.x - i);
+            if (sn + cnt > sp_max) return false;
+            const uint4 e = (uint32_t)lane < cnt ? rlog[i + lane] : make_uint4(0, 0, 0, 0);
+            for (uint32_t t = 0; t < cnt; ++t) {
+                const uint32_t id = __shfl_sync(kFull, e.x, t);
+                const uint32_t yb = __shfl_sync(kFull, e.y, t);
+                warp_push(sp, sn, make_uint2(id, yb ^ 0x80000000u), lane);  // -distance
+            }
+            i += cnt;
+        }
+        if (j < pops) {
+            if (sn == 0 || sp.get(0).x != pj.y) return false;
+            warp_pop(sp, sn, lane);
+        }
+    }
+    return true;
+}
+
 // Number of entries of the sorted values a[0, n) that are <= y.
 __device__ __forceinline__ uint32_t upper_rank(const float* a, uint32_t n, float y) {
     uint32_t lo = 0, hi = n;
@@ -154,14 +190,58 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
         }
         __syncwarp();
         uint32_t pops = 0, calcs = 1;
+        // Lazy mode: no search heap until a pop meets a tie. The heap's live
+        // entries (distance <= lowerBound; the others are never popped) are
+        // exactly the unpopped entries of the sorted pool, so while the
+        // smallest of them is unique it is the heap's top. `cur` is the first
+        // unpopped entry; pops are logged (pushes are the result log) so the
+        // heap can be rebuilt when the smallest distance is shared.
+        bool heap = !ra.lazy;
+        uint32_t cur = 0;
+        uint2* plg = ra.plog ? ra.plog + (size_t)qi * ra.rlog_cap : nullptr;
 
         while (!fail) {
             // qg.hpp:313-318
-            if (sn == 0) break;
-            const uint2 top = sp.get(0);
-            if (-__uint_as_float(top.y) > lower) break;
-            warp_pop(sp, sn, lane);
-            const uint32_t u = top.x;
+            uint32_t u;
+            if (heap) {
+                if (sn == 0) break;
+                const uint2 top = sp.get(0);
+                if (-__uint_as_float(top.y) > lower) break;
+                warp_pop(sp, sn, lane);
+                u = top.x;
+            } else {
+                if (cur >= alen) break;  // nothing live: top > lowerBound or empty
+                uint32_t nxt = alen;
+                for (uint32_t x0 = cur + 1; x0 < alen; x0 += 32) {
+                    const uint32_t x = x0 + lane;
+                    const unsigned um = __ballot_sync(kFull, x < alen && !(ai[x] & kPopped));
+                    if (um) {
+                        nxt = x0 + __ffs(um) - 1;
+                        break;
+                    }
+                }
+                if (nxt < alen && ad[nxt] == ad[cur]) {
+                    // equal smallest distances: the heap layout decides
+                    if (!rebuild_search_heap(sp, sn, sp_max, rlog, plg, acc_n, pops, lane)) {
+                        fail = true;
+                        break;
+                    }
+                    heap = true;
+                    continue;
+                }
+                if (pops >= ra.rlog_cap) {
+                    fail = true;
+                    break;
+                }
+                u = ai[cur];
+                __syncwarp();
+                if (lane == 0) {
+                    ai[cur] = u | kPopped;
+                    plg[pops] = make_uint2(acc_n, u);
+                }
+                __syncwarp();
+                cur = nxt;
+            }
             ++pops;
 
             // qg.hpp:320-324: unvisited neighbours in list order
@@ -210,7 +290,7 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
                     ub = upper_rank(ad, alen, y);
                     // a node the visited cache forgot: still pooled, same distance
                     for (uint32_t x = ub; x > 0 && ad[x - 1] == y; --x)
-                        if (ai[x - 1] == id) {
+                        if ((ai[x - 1] & ~kPopped) == id) {
                             mem = false;
                             break;
                         }
@@ -232,7 +312,7 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
                 const unsigned am = __ballot_sync(kFull, acc);
                 const uint32_t m = __popc(am);
                 if (m == 0) continue;
-                if (alen + m > acap || acc_n + m > ra.rlog_cap || sn + m > sp_max) {
+                if (alen + m > acap || acc_n + m > ra.rlog_cap || (heap && sn + m > sp_max)) {
                     fail = true;
                     break;
                 }
@@ -241,6 +321,7 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
                 // entry x moves up by the number of accepted j with ub_j <= x
                 uint32_t before = 0;
                 uint32_t ubmin = acap;
+                uint32_t shc = 0;   // lazy: accepted ones that go before entry `cur`
                 float pmax = -INF;  // largest accepted value up to this lane
                 {
                     unsigned bm = am;
@@ -251,6 +332,7 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
                         const uint32_t us = __shfl_sync(kFull, ub, s);
                         before += (ys < y || (ys == y && s < lane)) ? 1u : 0u;
                         ubmin = min(ubmin, us);
+                        shc += us <= cur ? 1u : 0u;
                         if (s <= lane) pmax = fmaxf(pmax, ys);
                     }
                 }
@@ -283,6 +365,9 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
                     ai[ub + before] = id;
                 }
                 __syncwarp();
+                // the first unpopped entry: the one at `cur` moved up, or an
+                // accepted one placed before it
+                cur = min(cur + shc, __reduce_min_sync(kFull, acc ? ub + before : 0xFFFFFFFFu));
                 alen += m;
                 const uint32_t acc_new = acc_n + m;
                 const float lf = ad[min(acc_new, ef) - 1];
@@ -308,7 +393,7 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
                 lower = lf;
                 acc_n = acc_new;
                 // the search pool takes them in list order (qg.hpp:332)
-                unsigned bm = am;
+                unsigned bm = heap ? am : 0u;
                 while (bm) {
                     const int s = __ffs(bm) - 1;
                     bm &= bm - 1;
@@ -338,10 +423,11 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
             if (direct) {
                 uint32_t* out = a.ids + (size_t)qi * a.kstride;
                 for (uint32_t x = lane; x < k - kk; x += 32) out[x] = kNoId;
-                for (uint32_t x = P - kk + lane; x < P; x += 32) out[x + k - P] = ai[x];
+                for (uint32_t x = P - kk + lane; x < P; x += 32)
+                    out[x + k - P] = ai[x] & ~kPopped;
                 if (a.pool_ids) {
                     for (uint32_t x = lane; x < a.pstride; x += 32) {
-                        a.pool_ids[(size_t)qi * a.pstride + x] = x < P ? ai[x] : kNoId;
+                        a.pool_ids[(size_t)qi * a.pstride + x] = x < P ? ai[x] & ~kPopped : kNoId;
                         a.pool_d[(size_t)qi * a.pstride + x] = x < P ? ad[x] : INF;
                     }
                 }

@@ -203,12 +203,13 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     const bool heap_all = t.mode == 2;
     cudaError_t e;
 
-    if (t.mode == 3 || t.mode == 4 || t.mode == 5) {
-        // replay (3), split (4) or batch (5) kernel over every query, then the
-        // result replay pass where the search warps do not replay in place, in
-        // chunks whose result logs fit 1 GiB; spilled queries go to the exact
-        // kernel
-        const bool batch = t.mode == 5;
+    if (t.mode >= 3) {
+        // replay (3), split (4) or batch (5; 6 with the lazy search heap)
+        // kernel over every query, then the result replay pass where the
+        // search warps do not replay in place, in chunks whose logs fit
+        // 1.5 GiB; spilled queries go to the exact kernel
+        const bool lazy = t.mode == 6;
+        const bool batch = t.mode == 5 || lazy;
         const bool split = t.mode == 4 || batch;
         const int RE = lqg::replay_pool_regs(b.ef0);
         if (RE == 0) return fail(LQG_ERR_ARG, "ef too large for the replay kernels");
@@ -221,10 +222,14 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         ra.rlog_cap = std::max(1024u, 16u * b.ef0);
         ra.replay_all = t.replay_all;
         ra.acap = 32u * (uint32_t)RE;
+        ra.lazy = lazy ? 1u : 0u;
         const int64_t chunk = std::min<int64_t>(
             b.m, std::max<int64_t>(1024, (int64_t(1) << 30) / ((int64_t)ra.rlog_cap * 16)));
         if ((s = grow(w.d_rlog, w.cap_rlog, (size_t)chunk * ra.rlog_cap)) != LQG_OK) return s;
         if ((s = grow(w.d_rlen, w.cap_rlen, (size_t)chunk)) != LQG_OK) return s;
+        if (lazy && (s = grow(w.d_plog, w.cap_plog, (size_t)chunk * ra.rlog_cap)) != LQG_OK)
+            return s;
+        ra.plog = lazy ? w.d_plog : nullptr;
         ra.rlog = w.d_rlog;
         ra.rlen = w.d_rlen;
         // split kernel blocks hold at most 5 warps (its 96-register budget)
@@ -716,7 +721,7 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         n.blocks_per_sm = t->blocks_per_sm;
     }
     if (t->mode) {
-        if (t->mode > 5) return fail(LQG_ERR_ARG, "mode must be 1, 2, 3, 4 or 5");
+        if (t->mode > 6) return fail(LQG_ERR_ARG, "mode must be in [1, 6]");
         n.mode = t->mode;
     }
     if (t->heap_warps) {
@@ -737,7 +742,7 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         return fail(LQG_ERR_ARG, "replay kernel tuning needs more than 227 KB of shared memory");
     if (n.mode == 4 && lqg::split_smem_bytes(ix->dim, n.visited_bits, n.heap_scap, 1) > 227 * 1024)
         return fail(LQG_ERR_ARG, "split kernel tuning needs more than 227 KB of shared memory");
-    if (n.mode == 5 && lqg::batch_smem_bytes(ix->dim, n.visited_bits, n.heap_scap,
+    if (n.mode >= 5 && lqg::batch_smem_bytes(ix->dim, n.visited_bits, n.heap_scap,
                                              32u * (uint32_t)lqg::replay_pool_regs(kMaxEf), 1) >
                            227 * 1024)
         return fail(LQG_ERR_ARG, "batch kernel tuning needs more than 227 KB of shared memory");

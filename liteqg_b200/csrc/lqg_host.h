@@ -60,6 +60,8 @@ struct Workspace {
     uint4* d_rlog = nullptr;       // replay kernel: per-query result logs
     uint32_t* d_rlen = nullptr;    // replay kernel: per-query log lengths
     size_t cap_rlog = 0, cap_rlen = 0;
+    uint2* d_plog = nullptr;       // batch kernel, lazy heap: per-query pop logs
+    size_t cap_plog = 0;
     size_t sp_global_slots = 0;    // warps covered
     int x_blocks = 0, x_warps_per_block = 4;
     float* d_q = nullptr;
@@ -82,7 +84,8 @@ struct Workspace {
         dfree(d_sp_global);
         dfree(d_rlog);
         dfree(d_rlen);
-        cap_rlog = cap_rlen = 0;
+        dfree(d_plog);
+        cap_rlog = cap_rlen = cap_plog = 0;
         sp_global_slots = 0;
         dfree(d_q);
         dfree(d_kq);

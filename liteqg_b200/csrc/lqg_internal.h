@@ -61,6 +61,8 @@ struct ReplayArgs {
     uint32_t replay_all; // split/batch kernels: replay every query's result heap (else
                          // only those whose output the heap layout decides)
     uint32_t acap;       // batch kernel: sorted-pool slots (>= efcap + 32)
+    uint32_t lazy;       // batch kernel: build the search heap only at the first tied pop
+    uint2* plog;         // [m][rlog_cap] (accepted before the pop, popped id) per pop
 };
 constexpr uint32_t kRlenDone = 0xFFFFFFFEu;  // rlen: output already written
 constexpr uint32_t kReplayLogN = 128;  // search-heap log ring entries (8 bytes) per search warp

@@ -10,7 +10,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mode", [1, 2, 4, 5])
+@pytest.mark.parametrize("mode", [1, 2, 4, 5, 6])
 def test_graph_replay_equals_eager(golden, mode):
     import torch
 

@@ -7,7 +7,9 @@ search heap from the log, checks each step, and answers when equal distances
 make the heap layout decide. Mode 4: each search warp runs the exact search
 heap itself and keeps only a sorted array for the bound. Mode 5: as mode 4,
 with the sorted pool in shared memory and every expansion's candidates
-accepted or rejected at once from a rank count. In all, the result
+accepted or rejected at once from a rank count. Mode 6: as mode 5 with no
+search heap until a pop meets equal smallest distances; the heap is then
+rebuilt from the logs, every replayed pop checked. In all, the result
 heap is replayed afterwards from a per-query log by one warp per query,
 which checks every acceptance and writes the output. Bar: ids, FP32 pools and
 pop counts bit-exact against the reference's golden outputs and the oracle;
@@ -32,8 +34,9 @@ def lqg():
 # (tuning mode, replay_all): the split kernel writes unambiguous outputs from
 # its sorted array; replay_all=1 sends every query through the checked result
 # replay pass instead, so both paths are covered.
-@pytest.fixture(params=[(3, 0), (4, 0), (4, 1), (5, 0), (5, 1)],
-                ids=["replay", "split", "split-replay-all", "batch", "batch-replay-all"])
+@pytest.fixture(params=[(3, 0), (4, 0), (4, 1), (5, 0), (5, 1), (6, 0), (6, 1)],
+                ids=["replay", "split", "split-replay-all", "batch", "batch-replay-all",
+                     "lazy", "lazy-replay-all"])
 def mode(request):
     return request.param
 
