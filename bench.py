@@ -589,7 +589,7 @@ def uneven_arm(args, w, name, device):
                          ef_ptr=e_dev.data_ptr(), k_ptr=k_dev.data_ptr(), stream=sh)
 
     best = None
-    for mode, g in ((4, 4), (4, 8), (2, 4), (1, 4)):
+    for mode, g in ((6, 2), (6, 4), (5, 2), (4, 4), (2, 2), (2, 4), (1, 4)):
         ix.set_tuning(mode=mode, lanes_per_cand=g, heap_warps=4, heap_scap=512, visited_bits=10)
         for _ in range(2):
             step()

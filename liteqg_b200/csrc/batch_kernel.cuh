@@ -42,6 +42,10 @@
 // before and is still in the sorted pool with the same id and distance, and
 // it is dropped there.
 //
+// Lazy mode (ReplayArgs::lazy) keeps no search heap while the smallest
+// unpopped distance is unique (the heap's top is then the sorted pool's first
+// unpopped entry) and rebuilds it from the logs at the first tie (below).
+//
 // A query whose search pool, sorted pool or log outgrows its capacity goes to
 // the exact global-memory kernel through the spill list.
 #pragma once
@@ -118,7 +122,16 @@ __device__ __forceinline__ uint32_t upper_rank(const float* a, uint32_t n, float
     return lo;
 }
 
-template <int G, int DEGW>
+// Code words in flight per lane in the distance batches (LW). Up to 256
+// dimensions, 16 keeps the kernel within its 96 registers without spills at
+// degree 32 (32 spilled and ran 13% slower) and larger degrees, which hold
+// more neighbour ids, take 8. Longer rows take 32: a 960-byte row fetched 8
+// words at a time needs dozens of dependent rounds, which costs more than the
+// spills.
+constexpr int batch_load_words(int degw) { return degw == 1 ? 16 : 8; }
+constexpr uint32_t kBatchWideDim = 256;
+
+template <int G, int DEGW, int LW>
 __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, ReplayArgs ra) {
     using namespace heapops;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -173,7 +186,7 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
         const uint32_t ep = a.entry;
         if (lane == 0) cid[0] = ep;
         __syncwarp();
-        eval_batch<G, G>(a, cid, cd, 0, 1, qs, pmin, pscale, g, r);
+        eval_batch<G, G, LW, 1>(a, cid, cd, 0, 1, qs, pmin, pscale, g, r);
         __syncwarp();
         const float d0 = cd[0];
         bool fail = !(d0 < INF);
@@ -266,7 +279,7 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
 
             // qg.hpp:325-328
             for (uint32_t b = 0; b < ncand; b += 32)
-                eval_batch<G, G>(a, cid, cd, b, ncand, qs, pmin, pscale, g, r);
+                eval_batch<G, G, LW, 1>(a, cid, cd, b, ncand, qs, pmin, pscale, g, r);
             calcs += ncand;
             __syncwarp();
 
@@ -455,12 +468,12 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
     }
 }
 
-template <int G, int DEGW>
+template <int G, int DEGW, int LW>
 static cudaError_t batch_run(const SearchArgs& a, const ReplayArgs& ra, int warps, int blocks,
                             cudaStream_t st, int* occ) {
     const size_t dpad = (a.dim + 15u) & ~15u;
     const size_t smem = 8 * dpad + (size_t)warps * batch_warp_bytes(a.dim, a.vbits, ra.scap, ra.acap);
-    auto k = batch_search_kernel<G, DEGW>;
+    auto k = batch_search_kernel<G, DEGW, LW>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, warps * 32, smem);
@@ -468,17 +481,24 @@ static cudaError_t batch_run(const SearchArgs& a, const ReplayArgs& ra, int warp
     return cudaGetLastError();
 }
 
-// All instances for one lanes-per-candidate G: degree words 1-4.
+// All instances for one lanes-per-candidate G: degree words 1-4, each with
+// the short and the long code-load window.
 template <int G>
 cudaError_t batch_dispatch(const SearchArgs& a, const ReplayArgs& ra, int degw, int warps,
                            int blocks, cudaStream_t st, int* occ) {
+    const bool wide = a.dim >= kBatchWideDim;
+#define LQG_BCASE(DW)                                                                   \
+    case DW:                                                                            \
+        return wide ? batch_run<G, DW, 32>(a, ra, warps, blocks, st, occ)               \
+                    : batch_run<G, DW, batch_load_words(DW)>(a, ra, warps, blocks, st, occ);
     switch (degw) {
-        case 1: return batch_run<G, 1>(a, ra, warps, blocks, st, occ);
-        case 2: return batch_run<G, 2>(a, ra, warps, blocks, st, occ);
-        case 3: return batch_run<G, 3>(a, ra, warps, blocks, st, occ);
-        case 4: return batch_run<G, 4>(a, ra, warps, blocks, st, occ);
+        LQG_BCASE(1)
+        LQG_BCASE(2)
+        LQG_BCASE(3)
+        LQG_BCASE(4)
         default: return cudaErrorInvalidValue;
     }
+#undef LQG_BCASE
 }
 
 }  // namespace lqg

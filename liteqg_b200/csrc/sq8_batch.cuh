@@ -40,8 +40,11 @@ __device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigne
 // Distances of candidates cid[base + p * (32/G) + g], p < NP, into cd[].
 // Lane r of group g owns accumulators [r*A, r*A + A) (A = 16/G); all code
 // bytes of a round of U chunks, for all NP passes, are requested before any
-// arithmetic. Passes with no valid candidate are skipped (warp-uniform).
-template <int G, int NP>
+// arithmetic: LW code words per lane in flight (U = LW / (NP * words per
+// chunk), at most 8). With PF, each round first asks L1 for the next round's
+// bytes of every row, so a row split over two rounds costs one trip to L2 or
+// HBM. Passes with no valid candidate are skipped (warp-uniform).
+template <int G, int NP, int LW = 32, int PF = 0>
 __device__ __forceinline__ void eval_batch(const SearchArgs& a, const uint32_t* cid, float* cd,
                                            uint32_t base, uint32_t ncand,
                                            const float* __restrict__ qs,
@@ -50,7 +53,7 @@ __device__ __forceinline__ void eval_batch(const SearchArgs& a, const uint32_t* 
     constexpr int A = 16 / G;
     constexpr int W = (A + 3) / 4;
     constexpr int CPP = 32 / G;
-    constexpr int UU = 32 / (NP * W);
+    constexpr int UU = LW / (NP * W);
     constexpr int U = UU < 1 ? 1 : (UU > 8 ? 8 : UU);
     constexpr int AP = A >= 2 ? A / 2 : 1;  // accumulator pairs
     const uint32_t dim = a.dim;
@@ -74,6 +77,12 @@ __device__ __forceinline__ void eval_batch(const SearchArgs& a, const uint32_t* 
         for (int t = 0; t < AP; ++t) acc2[p][t] = 0ull;
     }
     for (uint32_t b0 = 0; b0 < mul; b0 += 16 * U) {
+        if constexpr (PF != 0) {
+#pragma unroll
+            for (int p = 0; p < NP; ++p)
+                if (valid[p] && b0 + 16 * U < mul)
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(rowp[p] + b0 + 16 * U));
+        }
         uint32_t w[NP][U][W];
 #pragma unroll
         for (int p = 0; p < NP; ++p)
