@@ -10,8 +10,9 @@ recall@10 against an FP64 brute-force ground truth is >= 0.95. Synthetic data
 stands in for the reference's datasets (none ship with it).
 
 One "step" = one batched search of all 10,000 queries (one persistent launch
-of the fast kernel plus the exact kernel for tied queries), inputs resident in
-HBM. The L2 is flushed between steps (a 256 MiB write), outside the timed
+of the search kernel the autotuner picks, on this workload the batch kernel
+with the lazy search heap, plus the exact kernel over the queries that outgrew
+its capacities, usually none), inputs resident in HBM. The L2 is flushed between steps (a 256 MiB write), outside the timed
 events. `e2e` times the same step through the host-buffer C-ABI call
 (lqg_search_batch): pinned host queries in, ids out, inside the timed region.
 
@@ -637,6 +638,9 @@ def uneven_arm(args, w, name, device):
     print(json.dumps(line), flush=True)
 
 
+SERVING_STREAMS = 8  # batches in flight at once (each on its own stream)
+
+
 def serving_arm(args, w, name, device):
     """open-loop Poisson arrivals through the serving loop."""
     import torch
@@ -656,14 +660,43 @@ def serving_arm(args, w, name, device):
     n, dim, deg = w["n"], w["dim"], w["deg"]
     ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
     ix.load(path)
-    ix.set_tuning(mode=4, lanes_per_cand=4, heap_warps=4, heap_scap=512, visited_bits=10)
+    # kernel mode: the fastest on one 8,192-query batch of the request mix
+    # (every mode returns the same ids)
+    rng = np.random.default_rng(4)
+    mq = 8192
+    q_dev = torch.from_numpy(queries[:mq]).cuda(device)
+    k_dev = torch.from_numpy(rng.choice(w["k_choices"], mq).astype(np.uint32)).cuda(device)
+    e_dev = torch.from_numpy(rng.choice(w["ef_choices"], mq).astype(np.uint32)).cuda(device)
+    kmax, efmax = max(w["k_choices"]), max(w["ef_choices"])
+    ids = torch.empty((mq, kmax), dtype=torch.int32, device=q_dev.device)
+    stream = torch.cuda.current_stream(q_dev.device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=q_dev.device)
+
+    def step():
+        ix.search_device(q_dev.data_ptr(), mq, 0, ids.data_ptr(), kmax, ef=efmax,
+                         ef_ptr=e_dev.data_ptr(), k_ptr=k_dev.data_ptr(),
+                         stream=stream.cuda_stream)
+
+    best = None
+    for mode, g in ((6, 2), (5, 2), (4, 4), (2, 2), (2, 4)):
+        ix.set_tuning(mode=mode, lanes_per_cand=g, heap_warps=4, heap_scap=512, visited_bits=10)
+        step()
+        ix.stream_status(stream.cuda_stream)
+        ms = _timed(step, 3, flush, stream)
+        log(f"[serving] mode {mode} G {g}: {ms:.2f} ms per {mq} mixed requests")
+        if best is None or ms < best[0]:
+            best = (ms, mode, g)
+    ix.set_tuning(mode=best[1], lanes_per_cand=best[2], heap_warps=4, heap_scap=512,
+                  visited_bits=10)
+    del q_dev, k_dev, e_dev, ids, flush
     rec = {}
     for ef in w["ef_choices"]:
         _, (pid, _) = ix.search(sample, 10, ef=ef, return_pool=True)
         rec[int(ef)] = recall_at(pid, gt, 10)
     rng = np.random.default_rng(3)
     rows = []
-    with Server(ix, streams=4, max_k=max(w["k_choices"]), max_ef=max(w["ef_choices"])) as srv:
+    with Server(ix, streams=SERVING_STREAMS, max_k=max(w["k_choices"]),
+                max_ef=max(w["ef_choices"])) as srv:
         for rate in w["rates"]:
             m = int(min(len(queries), rate * w["seconds"]))
             arrivals = np.cumsum(rng.exponential(1e6 / rate, m))
@@ -694,7 +727,8 @@ def serving_arm(args, w, name, device):
         "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']}, open-loop "
                                f"Poisson arrivals, k from {list(w['k_choices'])}, ef from "
                                f"{list(w['ef_choices'])}", "recall_at_10_pool_by_ef": rec,
-                   "server": {"streams": 4}},
+                   "server": {"streams": SERVING_STREAMS, "mode": best[1],
+                              "lanes_per_cand": best[2]}},
         "serving": rows,
         "plain_qps": len(lat) / sum(lat), "plain_p50_ms": 1e3 * float(np.percentile(lat, 50)),
         "plain_p99_ms": 1e3 * float(np.percentile(lat, 99)),

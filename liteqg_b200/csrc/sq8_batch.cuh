@@ -102,12 +102,27 @@ __device__ __forceinline__ void eval_batch(const SearchArgs& a, const uint32_t* 
             if (b >= mul) break;
             const uint32_t d0 = b + r * A;
             if constexpr (A >= 2) {
+                // query, min and scale pairs: 16-byte loads where a lane owns
+                // 4 or more dimensions of the chunk (every caller's arrays
+                // start on 16 bytes, and d0 is a multiple of A)
                 unsigned long long q2[AP], m2[AP], s2[AP];
+                if constexpr (AP >= 2) {
 #pragma unroll
-                for (int t = 0; t < AP; ++t) {
-                    q2[t] = *reinterpret_cast<const unsigned long long*>(qs + d0 + 2 * t);
-                    m2[t] = *reinterpret_cast<const unsigned long long*>(pmin + d0 + 2 * t);
-                    s2[t] = *reinterpret_cast<const unsigned long long*>(pscale + d0 + 2 * t);
+                    for (int t = 0; t < AP; t += 2) {
+                        const ulonglong2 qq = *reinterpret_cast<const ulonglong2*>(qs + d0 + 2 * t);
+                        const ulonglong2 mm = *reinterpret_cast<const ulonglong2*>(pmin + d0 + 2 * t);
+                        const ulonglong2 ss = *reinterpret_cast<const ulonglong2*>(pscale + d0 + 2 * t);
+                        q2[t] = qq.x;
+                        q2[t + 1] = qq.y;
+                        m2[t] = mm.x;
+                        m2[t + 1] = mm.y;
+                        s2[t] = ss.x;
+                        s2[t + 1] = ss.y;
+                    }
+                } else {
+                    q2[0] = *reinterpret_cast<const unsigned long long*>(qs + d0);
+                    m2[0] = *reinterpret_cast<const unsigned long long*>(pmin + d0);
+                    s2[0] = *reinterpret_cast<const unsigned long long*>(pscale + d0);
                 }
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
