@@ -166,6 +166,16 @@ def recall_at(pool_ids, gt, k):
     return hits / (len(gt) * k)
 
 
+def coverage_at(pool_ids, gt, k):
+    """Share of the true k nearest found anywhere in the pool: with best-k
+    recall below it, the search reached the neighbours and the SQ8 distances
+    ordered them below others; with both low, the graph did not reach them."""
+    hits = 0
+    for i in range(len(gt)):
+        hits += len(set(pool_ids[i].tolist()) & set(gt[i, :k].tolist()))
+    return hits / (len(gt) * k)
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -576,6 +586,7 @@ def uneven_arm(args, w, name, device):
     # recall: best-10 of each query's pool (untimed)
     _, (pid, _) = ix.search(queries, 10, ef=efq, return_pool=True)
     rec_by_ef = {int(e): recall_at(pid[efq == e], gt[efq == e], 10) for e in w["ef_choices"]}
+    cov_by_ef = {int(e): coverage_at(pid[efq == e], gt[efq == e], 10) for e in w["ef_choices"]}
     dev = torch.device("cuda", device)
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
@@ -630,7 +641,8 @@ def uneven_arm(args, w, name, device):
         "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']}, {nq} queries, "
                                f"per-query ef from {list(w['ef_choices'])}, k from "
                                f"{list(w['k_choices'])} (seed 2)",
-                   "recall_at_10_pool_by_ef": rec_by_ef, "mode": best[1], "lanes_per_cand": best[2],
+                   "recall_at_10_pool_by_ef": rec_by_ef, "pool_coverage_at_10_by_ef": cov_by_ef,
+                   "mode": best[1], "lanes_per_cand": best[2],
                    "l2": "flushed between steps (256 MiB write)"},
         "graph_qps": nq / (graph_ms / 1e3), "graph_ids_equal": graph_ok,
         "gpu_launches": {1: 3, 2: 2, 4: 2}.get(best[1], 3) * K,
@@ -689,10 +701,11 @@ def serving_arm(args, w, name, device):
     ix.set_tuning(mode=best[1], lanes_per_cand=best[2], heap_warps=4, heap_scap=512,
                   visited_bits=10)
     del q_dev, k_dev, e_dev, ids, flush
-    rec = {}
+    rec, cov = {}, {}
     for ef in w["ef_choices"]:
         _, (pid, _) = ix.search(sample, 10, ef=ef, return_pool=True)
         rec[int(ef)] = recall_at(pid, gt, 10)
+        cov[int(ef)] = coverage_at(pid, gt, 10)
     rng = np.random.default_rng(3)
     rows = []
     with Server(ix, streams=SERVING_STREAMS, max_k=max(w["k_choices"]),
@@ -727,6 +740,7 @@ def serving_arm(args, w, name, device):
         "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']}, open-loop "
                                f"Poisson arrivals, k from {list(w['k_choices'])}, ef from "
                                f"{list(w['ef_choices'])}", "recall_at_10_pool_by_ef": rec,
+                   "pool_coverage_at_10_by_ef": cov,
                    "server": {"streams": SERVING_STREAMS, "mode": best[1],
                               "lanes_per_cand": best[2]}},
         "serving": rows,

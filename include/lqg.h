@@ -254,9 +254,13 @@ LQG_API lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t);
  * are on the GPU are admitted as contexts free up and overlap with them.
  * Each context holds the device state of at most `max_batch` requests
  * (query, k, ef, ids, plus its own work areas); max_batch defaults to what
- * `state_budget` bytes (default 256 MiB) allow. Results are exactly those of
- * a search of the query alone. While a server runs, use the index only
- * through it. */
+ * `state_budget` bytes (default 256 MiB) allow. Start runs one full-size
+ * batch on every context (max_batch queries at max_k and max_ef, in the
+ * index's current tuning mode) so that the contexts' work areas are at their
+ * largest before the first request: growing them later would allocate device
+ * memory, which waits for the whole device. Set the tuning before starting.
+ * Results are exactly those of a search of the query alone. While a server
+ * runs, use the index only through it. */
 typedef struct lqg_server lqg_server;
 typedef struct {
     uint32_t streams;      /* contexts (batches in flight), default 4 */

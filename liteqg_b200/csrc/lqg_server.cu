@@ -222,6 +222,30 @@ double percentile(std::vector<double> v, double p) {
     return v[i];
 }
 
+// One full-size batch (max_batch zero queries at max_k and max_ef, in the
+// index's current kernel mode) on context c before serving starts: the work
+// areas a batch grows to fit (result and pop logs, search-heap areas) reach
+// their largest size here. Growing them while serving would free and
+// allocate device memory, which waits for every stream of the device.
+lqg_status warm_context(lqg_server* s, Ctx& c) {
+    const uint32_t mb = s->cfg.max_batch;
+    const uint32_t dim = s->ix->dim;
+    std::memset(c.h_q, 0, (size_t)mb * dim * sizeof(float));
+    for (uint32_t i = 0; i < mb; ++i) {
+        c.h_k[i] = s->cfg.max_k;
+        c.h_ef[i] = s->cfg.max_ef;
+    }
+    LQG_CUDA(cudaMemcpyAsync(c.d_q, c.h_q, (size_t)mb * dim * 4, cudaMemcpyHostToDevice, c.st));
+    LQG_CUDA(cudaMemcpyAsync(c.d_k, c.h_k, (size_t)mb * 4, cudaMemcpyHostToDevice, c.st));
+    LQG_CUDA(cudaMemcpyAsync(c.d_ef, c.h_ef, (size_t)mb * 4, cudaMemcpyHostToDevice, c.st));
+    BatchSpec b{c.d_q, (int64_t)mb, c.d_k, 0, c.d_ef, s->cfg.max_ef, c.d_ids,
+                s->cfg.max_k, nullptr, nullptr, 0, nullptr, c.st};
+    const lqg_status st = run_batch(s->ix, c.ws, b, false);
+    if (st != LQG_OK) return st;
+    LQG_CUDA(cudaStreamSynchronize(c.st));
+    return LQG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -268,6 +292,14 @@ lqg_status lqg_server_start(lqg_index* ix, const lqg_server_config* cfg, lqg_ser
             for (auto& y : s->ctx) free_ctx(y, ix->device);
             delete s;
             return fail(LQG_ERR_NOMEM, "serving-loop context allocation failed");
+        }
+    }
+    for (auto& x : s->ctx) {
+        const lqg_status st = warm_context(s, x);
+        if (st != LQG_OK) {
+            for (auto& y : s->ctx) free_ctx(y, ix->device);
+            delete s;
+            return st;
         }
     }
     s->t_start = Clock::now();
