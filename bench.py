@@ -65,6 +65,11 @@ WORKLOADS = {
                          deg=64, efb=400, iters=3, random_edges=8, path_take=64, far_budget=8,
                          nq=4096, kind="uneven", ef_choices=(32, 64, 128, 256, 512),
                          k_choices=(1, 10, 100)),
+    # index build with BF16 tensor-core pruning against the
+    # FP32 prune (unit-length rows; centre entries N(0, 1), sigma 0.3)
+    "build-1m768": dict(n=1_000_000, dim=768, gen="gauss_mixture_unit", clusters=2048, sigma=0.3,
+                        deg=64, efb=400, iters=3, random_edges=8, path_take=64, far_budget=8,
+                        nq=2000, kind="build", ef=128),
     # serving loop, open-loop Poisson arrivals
     "serving-10m96": dict(n=10_000_000, dim=96, gen="gauss_mixture", clusters=4096, sigma=0.25,
                           deg=32, efb=300, iters=3, random_edges=8, path_take=64, far_budget=8,
@@ -84,7 +89,9 @@ def gen_data(w, which: str, rank: int = 0):
     if w["gen"] == "uniform":
         rng = np.random.default_rng(0 if which == "base" else 1 + 1000 * rank)
         return rng.random((n, w["dim"]), dtype=np.float32)
-    if w["gen"] == "gauss_mixture":  # centre entries N(0, 1), isotropic sigma, float
+    if w["gen"] in ("gauss_mixture", "gauss_mixture_unit"):
+        # centre entries N(0, 1), isotropic sigma, float; "_unit": rows scaled
+        # to unit L2 norm
         centres = np.random.default_rng(0).normal(0.0, 1.0, (w["clusters"], w["dim"]))
         rng = np.random.default_rng(100 if which == "base" else 1 + 1000 * rank)
         out = np.empty((n, w["dim"]), dtype=np.float32)
@@ -92,7 +99,10 @@ def gen_data(w, which: str, rank: int = 0):
         for s in range(0, n, step):
             m = min(step, n - s)
             lab = rng.integers(0, w["clusters"], m)
-            out[s:s + m] = centres[lab] + rng.normal(0.0, w["sigma"], (m, w["dim"]))
+            x = centres[lab] + rng.normal(0.0, w["sigma"], (m, w["dim"]))
+            if w["gen"] == "gauss_mixture_unit":
+                x /= np.linalg.norm(x, axis=1, keepdims=True)
+            out[s:s + m] = x
         return out
     centres = np.random.default_rng(0).uniform(w["lo"], w["hi"], (w["clusters"], w["dim"]))
     rng = np.random.default_rng(100 if which == "base" else 1 + 1000 * rank)
@@ -750,6 +760,92 @@ def serving_arm(args, w, name, device):
     print(json.dumps(line), flush=True)
 
 
+def build_arm(args, w, name, device):
+    """the same data built twice, with the BF16 tensor-core
+    prune (pair_kernel 1) and with the FP32 prune (pair_kernel 0); reports the
+    build times, the share of pruned edges that differ, recall@10 (best 10 of
+    the pool) of the queries at the workload's ef on both indexes, and the
+    error of the two distance forms against FP64 on sampled candidate sets."""
+    import torch
+
+    import liteqg_b200
+
+    torch.cuda.set_device(device)
+    base = gen_data(w, "base")
+    queries = gen_data(w, "query")
+    n, dim, deg, ef = w["n"], w["dim"], w["deg"], w["ef"]
+    res, graphs = {}, {}
+    for label, pk in (("bf16_tensor_core", 1), ("fp32", 0)):
+        ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
+        t = time.perf_counter()
+        rep = ix.build_index(base, w["efb"], num_iter=w["iters"], random_edges=w["random_edges"],
+                             path_take=w["path_take"], far_budget=w["far_budget"], pair_kernel=pk)
+        wall = time.perf_counter() - t
+        _, (pid, _) = ix.search(queries, 10, ef=ef, return_pool=True)
+        graphs[label] = ix.get_arrays()[2]
+        res[label] = {"build_s": wall, "report": rep, "pool": pid}
+        ix.close()
+        log(f"[build] {label}: {wall:.1f}s {rep}")
+    gt = ground_truth(name, w, base, queries, device, 0)
+    for label in res:
+        res[label]["recall_at_10"] = recall_at(res[label].pop("pool"), gt, 10)
+
+    def edges(nb):
+        src = np.repeat(np.arange(n, dtype=np.int64), deg)
+        dst = nb.reshape(-1).astype(np.int64)
+        ok = dst < n
+        return np.unique(src[ok] * n + dst[ok])
+
+    ea, eb = edges(graphs["bf16_tensor_core"]), edges(graphs["fp32"])
+    common = np.intersect1d(ea, eb, assume_unique=True).size
+    disagree = 1.0 - common / max(1, ea.size)
+
+    # distance error against FP64 on the neighbour sets of sampled nodes (the
+    # sets the prune compares), emulated with torch: BF16-rounded rows centred
+    # on the set's mean, exact products summed in FP32, FP32 norms (the tensor
+    # core form), and the FP32 sum of squared differences (the FP32 prune)
+    rng = np.random.default_rng(5)
+    dev = torch.device("cuda", device)
+    nb = graphs["bf16_tensor_core"]
+    rel_tc, rel_32 = [], []
+    for u in rng.choice(n, 500, replace=False):
+        ids = nb[u][nb[u] < n]
+        x = torch.from_numpy(base[ids]).to(dev)
+        x64 = x.double()
+        d64 = torch.cdist(x64, x64) ** 2
+        c = x - x.mean(0, keepdim=True)
+        cb = c.bfloat16().float()
+        nrm = (c * c).sum(1)
+        dtc = nrm[:, None] + nrm[None, :] - 2.0 * (cb @ cb.T)
+        d32 = ((x[:, None, :] - x[None, :, :]) ** 2).sum(2)
+        iu = torch.triu_indices(len(ids), len(ids), 1, device=dev)
+        ref = d64[iu[0], iu[1]]
+        rel_tc.append(((dtc.double()[iu[0], iu[1]] - ref).abs() / ref).cpu().numpy())
+        rel_32.append(((d32.double()[iu[0], iu[1]] - ref).abs() / ref).cpu().numpy())
+    rel_tc, rel_32 = np.concatenate(rel_tc), np.concatenate(rel_32)
+
+    tc = res["bf16_tensor_core"]
+    line = {
+        "metric": "index build: nodes/s with the BF16 tensor-core prune", "value": n / tc["build_s"],
+        "unit": "nodes/s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * tc["build_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (prune Gram), f32",
+        "data": "synthetic",
+        "config": {"workload": f"{name}: N={n} D={dim} unit-length rows from a Gaussian mixture of "
+                               f"{w['clusters']} clusters (sigma {w['sigma']}), deg={deg}, EF={w['efb']}, "
+                               f"{w['iters']} rounds; {w['nq']} queries, recall@10 at ef={ef}"},
+        "builds": res,
+        "pruned_edge_disagreement": disagree, "edges": int(ea.size),
+        "distance_rel_error_vs_fp64": {
+            "pairs": int(rel_tc.size), "sample": "all pairs of the final neighbour lists of 500 nodes "
+                                                 "(emulated on the GPU with torch)",
+            "bf16_gram": {"median": float(np.median(rel_tc)), "p99": float(np.percentile(rel_tc, 99)),
+                          "max": float(rel_tc.max())},
+            "fp32": {"median": float(np.median(rel_32)), "p99": float(np.percentile(rel_32, 99)),
+                     "max": float(rel_32.max())}},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def build_only(w, name, device):
     """One GPU build of the workload's index inside an NVTX range 'lqg_build'
     (the range a profiler filters on); prints the build report as JSON."""
@@ -804,7 +900,9 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                              device_id=torch.device("cuda", local))
     try:
-        if w.get("kind") == "uneven":
+        if w.get("kind") == "build":
+            build_arm(args, w, args.workload, local)
+        elif w.get("kind") == "uneven":
             uneven_arm(args, w, args.workload, local)
         elif w.get("kind") == "serving":
             serving_arm(args, w, args.workload, local)
