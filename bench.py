@@ -78,6 +78,12 @@ WORKLOADS = {
 }
 
 
+# a launch shape per kernel mode for --mode: (mode, lanes_per_cand,
+# visited_bits, warps_per_block, heap_warps, heap_scap)
+FIXED_TUNING = {1: (1, 4, 10, 8, 4, 1024), 2: (2, 4, 10, 8, 4, 1024), 3: (3, 4, 10, 8, 4, 512),
+                4: (4, 4, 10, 8, 4, 256), 5: (5, 2, 10, 8, 4, 256), 6: (6, 2, 10, 8, 4, 256)}
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -397,9 +403,16 @@ def gpu_arm(args, w, name, rank, world, device):
     # on the whole batch; every setting gives the same ids
     from liteqg_b200 import autotune
 
-    tuned = autotune.tune(ix, queries, chosen, k, path=None, device=device)
-    mode = tuned["mode"]
-    mode_ms = {str(c): t for t, c in tuned["all"]}
+    if args.mode:
+        # one fixed kernel mode (to time or profile that kernel)
+        c = FIXED_TUNING[args.mode]
+        ix.set_tuning(mode=c[0], lanes_per_cand=c[1], visited_bits=c[2], warps_per_block=c[3],
+                      heap_warps=c[4], heap_scap=c[5])
+        mode, mode_ms = args.mode, {str(list(c)): None}
+    else:
+        tuned = autotune.tune(ix, queries, chosen, k, path=None, device=device)
+        mode = tuned["mode"]
+        mode_ms = {str(c): t for t, c in tuned["all"]}
     if args.profile:
         torch.cuda.synchronize(dev)
         torch.cuda.nvtx.range_push("lqg_profile")
@@ -876,6 +889,8 @@ def main():
     ap.add_argument("--workload", default="batched-1m128", choices=sorted(WORKLOADS))
     ap.add_argument("--profile", type=int, default=0,
                     help="run N batched steps inside an NVTX range 'lqg_profile' and exit")
+    ap.add_argument("--mode", type=int, default=0, choices=sorted(FIXED_TUNING),
+                    help="use this kernel mode (see lqg_tuning) instead of the autotuner's choice")
     ap.add_argument("--build-only", action="store_true",
                     help="build the workload's index (no cache), print the build report, exit")
     args = ap.parse_args()
