@@ -52,7 +52,7 @@ LQG_API const char* lqg_last_error(void);
 
 /* Index(index_type, metric, num_elements, dimension, degree_bound):
  * python/bindings.cpp:38-61. index_type must be "QG", metric "L2",
- * degree_bound a positive multiple of 32 (32 or 64 run on the GPU), and
+ * degree_bound a positive multiple of 32 (up to 128 on the GPU), and
  * dimension in [33, 2048] (the reference's rotator aborts outside it,
  * symqglib/utils/rotator.hpp:55-76). device: CUDA ordinal. */
 LQG_API lqg_status lqg_create(const char* index_type, const char* metric,
