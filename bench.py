@@ -555,9 +555,11 @@ def gpu_arm(args, w, name, rank, world, device):
         "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": int(nq * dim * 4),
                 "d2h_bytes_per_step": int(nq * k * 4)},
         # kernels per batched step: fast + heap + exact (1), heap + exact (2),
-        # replay + result replay + exact (3), split or batch + exact (4-6); the
-        # L2 flush is torch's
-        "gpu_launches": {1: 3, 2: 2, 3: 3, 4: 2, 5: 2, 6: 2}.get(mode, 3) * K,
+        # per step: the work order (entry-distance kernel + 4 radix-sort
+        # passes compiled into the library from CUB), then fast + heap + exact
+        # (1), heap + exact (2), replay + result replay + exact (3), split or
+        # batch + exact (4-6); the L2 flush is torch's
+        "gpu_launches": (5 + {1: 3, 2: 2, 3: 3, 4: 2, 5: 2, 6: 2}.get(mode, 3)) * K,
         "clocks": clk.summary(),
         "p50_ms": statistics.median(step_ms), "p99_ms": float(np.percentile(step_ms, 99)),
         **extra,

@@ -227,6 +227,9 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             b.m, std::max<int64_t>(1024, (int64_t(1) << 30) / ((int64_t)ra.rlog_cap * 16)));
         if ((s = grow(w.d_rlog, w.cap_rlog, (size_t)chunk * ra.rlog_cap)) != LQG_OK) return s;
         if ((s = grow(w.d_rlen, w.cap_rlen, (size_t)chunk)) != LQG_OK) return s;
+        // longest-expected queries first (plain single-query calls keep theirs)
+        const bool order = !plain && b.m > 1;
+        if (order && (s = ensure_order(w, chunk)) != LQG_OK) return s;
         if (lazy && (s = grow(w.d_plog, w.cap_plog, (size_t)chunk * ra.rlog_cap)) != LQG_OK)
             return s;
         ra.plog = lazy ? w.d_plog : nullptr;
@@ -295,6 +298,9 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             }
             if (c.stats) c.stats += off * 4;
             c.m = mc;
+            if (order && mc > 1 &&
+                (s = order_queries(ix, w, c.queries, c.efq, mc, b.st, &c.qlist)) != LQG_OK)
+                return s;
             const int cb = (int)std::min<int64_t>(rb, (mc + sw - 1) / sw);
             e = launch(c, cb, nullptr);
             if (e != cudaSuccess) return cuda_fail(e, "search launch");
@@ -317,6 +323,13 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         return LQG_OK;
     } else {
 
+    // work order of the batch: longest-expected queries first
+    const int32_t* order = nullptr;
+    if (!plain && b.m > 1) {
+        if ((s = ensure_order(w, b.m)) != LQG_OK) return s;
+        if ((s = order_queries(ix, w, b.q, b.efq, b.m, b.st, &order)) != LQG_OK) return s;
+    }
+
     // 1. fast kernel over every query (mode 1); tied queries go to the list
     if (!heap_all) {
         SearchArgs a = base_args(ix, w, b);
@@ -327,6 +340,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         a.ties_ok = b.ties_ok;
         a.path = b.path;
         a.path_stride = b.path_stride;
+        a.qlist = order;
         int warps = plain ? 1 : (int)t.warps_per_block;
         int blocks = 1;
         if (!plain) {
@@ -349,6 +363,8 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         if (!heap_all) {
             h.qlist = w.d_flagged;
             h.nlist = w.d_ctl + kCtlFlagged;
+        } else {
+            h.qlist = order;
         }
         h.qhead = w.d_ctl + kCtlHeapHead;
         h.vbits = t.visited_bits;

@@ -62,6 +62,10 @@ struct Workspace {
     size_t cap_rlog = 0, cap_rlen = 0;
     uint2* d_plog = nullptr;       // batch kernel, lazy heap: per-query pop logs
     size_t cap_plog = 0;
+    uint32_t* d_okey = nullptr;    // work order: keys and query indices, in and out
+    int32_t* d_oidx = nullptr;     //   (4 x chunk entries each)
+    unsigned char* d_otemp = nullptr;  // work order: radix-sort scratch
+    size_t cap_okey = 0, cap_oidx = 0, cap_otemp = 0;
     size_t sp_global_slots = 0;    // warps covered
     int x_blocks = 0, x_warps_per_block = 4;
     float* d_q = nullptr;
@@ -86,6 +90,10 @@ struct Workspace {
         dfree(d_rlen);
         dfree(d_plog);
         cap_rlog = cap_rlen = cap_plog = 0;
+        dfree(d_okey);
+        dfree(d_oidx);
+        dfree(d_otemp);
+        cap_okey = cap_oidx = cap_otemp = 0;
         sp_global_slots = 0;
         dfree(d_q);
         dfree(d_kq);
@@ -190,6 +198,11 @@ struct lqg_index {
 namespace lqg_host {
 lqg_status check_batch(lqg_index* ix, BatchSpec& b);
 lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain);
+// Work order of a batch (order.cu): largest ef, then farthest from the entry
+// point, first.
+lqg_status ensure_order(Workspace& w, int64_t chunk);
+lqg_status order_queries(const lqg_index* ix, Workspace& w, const float* queries,
+                         const uint32_t* efq, int64_t m, cudaStream_t st, const int32_t** list);
 lqg_status search_host(lqg_index* ix, Workspace& w, const float* queries, int64_t m,
                        const uint32_t* k, uint32_t k0, const uint32_t* ef, uint32_t efb,
                        uint32_t* ids, uint32_t kstride, uint32_t* pool_ids, float* pool_d,
