@@ -227,9 +227,6 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             b.m, std::max<int64_t>(1024, (int64_t(1) << 30) / ((int64_t)ra.rlog_cap * 16)));
         if ((s = grow(w.d_rlog, w.cap_rlog, (size_t)chunk * ra.rlog_cap)) != LQG_OK) return s;
         if ((s = grow(w.d_rlen, w.cap_rlen, (size_t)chunk)) != LQG_OK) return s;
-        // longest-expected queries first (plain single-query calls keep theirs)
-        const bool order = !plain && b.m > 1;
-        if (order && (s = ensure_order(w, chunk)) != LQG_OK) return s;
         if (lazy && (s = grow(w.d_plog, w.cap_plog, (size_t)chunk * ra.rlog_cap)) != LQG_OK)
             return s;
         ra.plog = lazy ? w.d_plog : nullptr;
@@ -268,6 +265,10 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             const int64_t need = (chunk + sw - 1) / sw;
             if (need < rb) rb = (int)need;
         }
+        // longest-expected queries first, when a chunk holds more queries
+        // than the launch has warps (otherwise they all start at once)
+        const bool order = !plain && chunk > (int64_t)rb * sw;
+        if (order && (s = ensure_order(w, chunk)) != LQG_OK) return s;
         const size_t slots = (size_t)rb * sw;
         if (w.sp_global_slots < slots) {
             dfree(w.d_sp_global);
@@ -298,7 +299,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
             }
             if (c.stats) c.stats += off * 4;
             c.m = mc;
-            if (order && mc > 1 &&
+            if (order && mc > (int64_t)rb * sw &&
                 (s = order_queries(ix, w, c.queries, c.efq, mc, b.st, &c.qlist)) != LQG_OK)
                 return s;
             const int cb = (int)std::min<int64_t>(rb, (mc + sw - 1) / sw);
@@ -325,7 +326,9 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
 
     // work order of the batch: longest-expected queries first
     const int32_t* order = nullptr;
-    if (!plain && b.m > 1) {
+    // (only when the batch is larger than about one wave of resident warps;
+    // smaller batches start all their queries at once)
+    if (!plain && b.m > (int64_t)ix->num_sms * 16) {
         if ((s = ensure_order(w, b.m)) != LQG_OK) return s;
         if ((s = order_queries(ix, w, b.q, b.efq, b.m, b.st, &order)) != LQG_OK) return s;
     }

@@ -181,3 +181,35 @@ def test_replay_larger_index_uneven_batch(lqg, tmp_path, mode, dim, deg, integer
         assert np.array_equal(got, w.compat), (ef, k)
         assert np.array_equal(pd, w.pool_d), (ef, k)
         assert np.array_equal(pid, w.pool_ids), (ef, k)
+
+
+@pytest.mark.parametrize("work_mode", [2, 6])
+def test_large_batch_work_order(lqg, tmp_path, work_mode):
+    """8,000 queries (more than the launch's resident warps, so the batch is
+    reordered longest-expected first) with per-query ef and k: ids and pops
+    equal the oracle's, query by query, in the heap kernel's path (mode 2) and
+    the batch kernel's (mode 6)."""
+    from oracle.oracle import sq8_quantize
+
+    rng = np.random.default_rng(77)
+    n, dim, deg = 6000, 64, 32
+    cent = rng.uniform(0, 255, (32, dim))
+    gen = lambda m: np.clip(np.rint(cent[rng.integers(0, 32, m)] + rng.normal(0, 20, (m, dim))),
+                            0, 255).astype(np.float32)
+    x = gen(n)
+    codes, params = sq8_quantize(x, 2)
+    arr = IndexArrays(n, dim, deg, int(rng.integers(0, n)), x, _knn_graph(x, deg), codes, params)
+    path = str(tmp_path / "wo.idx")
+    write_index(path, arr)
+    ix = lqg.Index("QG", "L2", n, dim, deg)
+    ix.load(path)
+    ix.set_tuning(mode=work_mode)
+    q = gen(8000)
+    efq = rng.choice([10, 32, 64, 128], size=len(q)).astype(np.uint32)
+    kq = rng.choice([1, 10], size=len(q)).astype(np.uint32)
+    ids, st = _device(ix, q, 128, 10, kq=kq, efq=efq)
+    want = Oracle(arr).search(q, kq.astype(np.int32), efq.astype(np.int32))
+    for i in range(len(q)):
+        k = int(kq[i])
+        assert np.array_equal(ids[i, :k], want.compat[i, :k]), (i, efq[i], k)
+    assert np.array_equal(st[:, 0], want.pops)
