@@ -391,6 +391,11 @@ def gpu_arm(args, w, name, rank, world, device):
     st_fast = torch.zeros((nq, 4), dtype=torch.int32, device=dev)
     ix.search_device(q_dev.data_ptr(), nq, k, ids_x.data_ptr(), k, ef=chosen,
                      stats_ptr=st.data_ptr(), stream=sh, exact=True)
+    # mode 1 (fast kernel, heap kernel for tied queries): its tie flags give the
+    # share of queries that meet equal distances
+    c1 = FIXED_TUNING[1]
+    ix.set_tuning(mode=c1[0], lanes_per_cand=c1[1], visited_bits=c1[2], warps_per_block=c1[3],
+                  heap_warps=c1[4], heap_scap=c1[5])
     ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=chosen,
                      stats_ptr=st_fast.data_ptr(), stream=sh)
     ix.stream_status(sh)

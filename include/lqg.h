@@ -204,7 +204,9 @@ LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
                                            uint32_t pstride, uint32_t* stats,
                                            void* stream);
 
-/* Launch shape and policy. 0 fields keep the current value.
+/* Launch shape and policy. 0 fields keep the current value. A new index
+ * starts with mode 6, lanes_per_cand 2, visited_bits 10, warps_per_block 8,
+ * heap_warps 4, heap_scap 256.
  *   lanes_per_cand  {1,2,4,8,16}: lanes sharing one distance (both kernels)
  *   visited_bits    [8, 13]: slots of the per-query visited cache (2^bits)
  *   warps_per_block {1..16} and blocks_per_sm {1..32}: fast kernel shape

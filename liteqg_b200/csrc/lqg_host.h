@@ -179,7 +179,9 @@ struct lqg_index {
     lqg_host::Workspace ws;  // the default work area (one batch at a time)
 
     cudaStream_t own_stream = nullptr;
-    lqg_tuning tune{4, 10, 8, 0, 1, 4, 1024, 15, 0};
+    // default: the batch kernel with the lazy search heap (mode 6), the
+    // fastest on the bench batch and for single queries
+    lqg_tuning tune{2, 10, 8, 0, 6, 4, 256, 15, 0};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // recorded around the fast kernel
 
     ~lqg_index() {

@@ -20,8 +20,11 @@ def lqg():
 
 
 def open_index(lqg, g):
+    """An index on the fast kernel's path (tuning mode 1: fast kernel, heap
+    kernel for tied queries, exact kernel for capacity spills)."""
     ix = lqg.Index("QG", "L2", g["n"], g["dim"], g["deg"])
     ix.load(g["path"])
+    ix.set_tuning(mode=1, lanes_per_cand=4, heap_scap=1024)
     return ix
 
 
@@ -170,6 +173,7 @@ def test_larger_index_matches_oracle(lqg, tmp_path, dim, deg):
     write_index(path, arr)
     ix = lqg.Index("QG", "L2", n, dim, deg)
     ix.load(path)
+    ix.set_tuning(mode=1, lanes_per_cand=4, heap_scap=1024)
     o = Oracle(arr)
     q = np.clip(np.rint(cent[rng.integers(0, 64, 400)] + rng.normal(0, 20, (400, dim))), 0, 255).astype(np.float32)
     for ef, k in ((64, 10), (128, 100), (256, 10)):
