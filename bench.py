@@ -524,9 +524,20 @@ def gpu_arm(args, w, name, rank, world, device):
         fn, kind, keep = cpu_reference_search(path, w, queries, k, chosen, nthreads)
         cpu_qps, m, dt, cpu_ids = time_cpu(fn, queries, budget_s=8.0)
         ref_mismatch = int((cpu_ids[:m] != ids.cpu().numpy().view(np.uint32)[:m]).any(1).sum())
+        # one host thread, one query per call (the reference's own timing
+        # loop, reproduce/run.py:90-95)
+        fn1, _, keep1 = cpu_reference_search(path, w, queries, k, chosen, 1)
+        one = []
+        for i in range(min(300, nq)):
+            t = time.perf_counter()
+            fn1(queries[i:i + 1])
+            one.append(time.perf_counter() - t)
         cpu = {"value": cpu_qps, "unit": "queries/s", "cores": nthreads, "kind": kind,
                "sample": f"first {m} of {nq} queries, k={k}, ef={chosen}, {dt:.1f}s wall",
-               "ids_mismatch_vs_gpu": ref_mismatch}
+               "ids_mismatch_vs_gpu": ref_mismatch,
+               "single_thread_per_call": {"queries": len(one),
+                                          "p50_ms": 1e3 * float(np.median(one)),
+                                          "qps": len(one) / sum(one)}}
     else:
         cpu = None
 
