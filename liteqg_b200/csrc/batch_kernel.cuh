@@ -263,18 +263,33 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
             uint32_t v[DEGW];
 #pragma unroll
             for (int w = 0; w < DEGW; ++w) v[w] = __ldg(nb + w * 32 + lane);
+            // A list of degree > 32 spans DEGW words. Repeats inside a word
+            // are caught by match_any; a repeat of an id kept by an earlier
+            // word is caught by the cache, unless another id kept in this
+            // expansion took its slot: then (rare) later words also compare
+            // against the ids already kept, so no node is a candidate twice
+            // (qg.hpp:321). The duplicate check of the acceptance step only
+            // sees the pool from before this expansion.
+            bool lost = false;
 #pragma unroll
             for (int w = 0; w < DEGW; ++w) {
                 const uint32_t h = hash_id(v[w], vbits);
                 const bool seen = vis[h] == v[w];
                 const unsigned mm = __match_any_sync(kFull, v[w]);
-                const bool keep = !seen && (mm & lt) == 0;
+                bool keep = !seen && (mm & lt) == 0;
+                if (DEGW > 1 && w > 0 && lost && keep)
+                    for (uint32_t j = 0; j < ncand; ++j)
+                        if (cid[j] == v[w]) {
+                            keep = false;
+                            break;
+                        }
                 __syncwarp();
                 if (keep) vis[h] = v[w];
                 const unsigned kb = __ballot_sync(kFull, keep);
                 if (keep) cid[ncand + __popc(kb & lt)] = v[w];
                 ncand += __popc(kb);
                 __syncwarp();
+                if (DEGW > 1 && w + 1 < DEGW) lost = lost || __any_sync(kFull, keep && vis[h] != v[w]);
             }
 
             // qg.hpp:325-328

@@ -213,3 +213,41 @@ def test_large_batch_work_order(lqg, tmp_path, work_mode):
         k = int(kq[i])
         assert np.array_equal(ids[i, :k], want.compat[i, :k]), (i, efq[i], k)
     assert np.array_equal(st[:, 0], want.pops)
+
+
+@pytest.mark.parametrize("fix_mode", [5, 6])
+def test_repeated_ids_across_list_words(lqg, tmp_path, fix_mode):
+    """Degree 64 (two 32-id words per list) with ids repeated across the words
+    and a 256-slot visited cache, so a kept id's slot is often taken by
+    another id of the same expansion: every node is still a candidate once
+    per expansion, as the reference's visited set makes it (ids, pools and
+    pops equal the oracle's)."""
+    from oracle.oracle import sq8_quantize
+
+    rng = np.random.default_rng(64)
+    n, dim, deg = 5000, 64, 64
+    cent = rng.uniform(0, 255, (16, dim))
+    gen = lambda m: np.clip(np.rint(cent[rng.integers(0, 16, m)] + rng.normal(0, 25, (m, dim))),
+                            0, 255).astype(np.float32)
+    x = gen(n)
+    nb = _knn_graph(x, deg)
+    # the second word repeats a third of the first word's ids at random slots
+    for i in range(n):
+        src = rng.choice(32, 11, replace=False)
+        dst = 32 + rng.choice(32, 11, replace=False)
+        nb[i, dst] = nb[i, src]
+    codes, params = sq8_quantize(x, 2)
+    arr = IndexArrays(n, dim, deg, int(rng.integers(0, n)), x, nb, codes, params)
+    path = str(tmp_path / "rep.idx")
+    write_index(path, arr)
+    ix = lqg.Index("QG", "L2", n, dim, deg)
+    ix.load(path)
+    ix.set_tuning(mode=fix_mode, visited_bits=8)
+    o = Oracle(arr)
+    q = gen(300)
+    for ef in (32, 128):
+        want = o.search(q, 10, ef)
+        ids, (pid, pd), st = ix.search(q, 10, ef=ef, return_pool=True, return_stats=True)
+        assert np.array_equal(ids, want.compat), ef
+        assert np.array_equal(pd, want.pool_d), ef
+        assert np.array_equal(st[:, 0], want.pops), ef
