@@ -215,13 +215,13 @@ def test_large_batch_work_order(lqg, tmp_path, work_mode):
     assert np.array_equal(st[:, 0], want.pops)
 
 
-@pytest.mark.parametrize("fix_mode", [5, 6])
+@pytest.mark.parametrize("fix_mode", [1, 2, 4, 5, 6])
 def test_repeated_ids_across_list_words(lqg, tmp_path, fix_mode):
     """Degree 64 (two 32-id words per list) with ids repeated across the words
     and a 256-slot visited cache, so a kept id's slot is often taken by
     another id of the same expansion: every node is still a candidate once
     per expansion, as the reference's visited set makes it (ids, pools and
-    pops equal the oracle's)."""
+    pops equal the oracle's), in every kernel mode."""
     from oracle.oracle import sq8_quantize
 
     rng = np.random.default_rng(64)
