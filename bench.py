@@ -505,6 +505,18 @@ def gpu_arm(args, w, name, rank, world, device):
         b.synchronize()
         extra["qps_k100"] = nq * 5 / (a.elapsed_time(b) / 1e3)
         extra["k100_ef"] = max(chosen, w["k_extra"])
+        # the same search on a 4x larger batch (these queries and three more
+        # query seeds of the workload), L2 flushed: the kernel's throughput
+        # with less of the batch's ramp and tail per query
+        q4 = torch.from_numpy(np.concatenate([queries] + [gen_data(w, "query", r)
+                                                          for r in (1, 2, 3)])).to(dev)
+        ids4 = torch.empty((len(q4), k), dtype=torch.int32, device=dev)
+        for _ in range(2):
+            ix.search_device(q4.data_ptr(), len(q4), k, ids4.data_ptr(), k, ef=chosen, stream=sh)
+        t4 = _timed(lambda: ix.search_device(q4.data_ptr(), len(q4), k, ids4.data_ptr(), k,
+                                             ef=chosen, stream=sh), 5, flush, stream)
+        extra["large_batch"] = {"queries": len(q4), "ms": t4, "qps": len(q4) / (t4 / 1e3)}
+        del q4, ids4
         # plain: one query per launch through Index.search (the reference call form)
         P = min(1000, nq)
         lat = []
