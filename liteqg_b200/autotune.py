@@ -1,12 +1,12 @@
 """Autotuner for the search kernels' launch shape and policy.
 
 Times a small grid of `lqg_tuning` settings (kernel mode: 1 fast + heap for
-tied queries, 2 heap, 4 split, 5 batch, 6 batch with a lazy search heap; lanes per candidate, visited-cache size, warps
-per block, shared-memory search-pool slots) on a
-sample of the caller's queries with CUDA events, keeps the fastest, and caches
-the choice in a JSON file keyed on (N, D, degree, ef, k), so later runs on the
-same kind of index start from it. Every setting returns the same ids (the
-kernels are exact under all of them); only time differs.
+tied queries, 2 heap, 4 split, 5 batch, 6 batch with a lazy search heap;
+lanes per candidate, visited-cache size, warps per block, shared-memory
+search-pool slots) on the caller's queries with CUDA events, keeps the
+fastest, and caches the choice in a JSON file keyed on (N, D, degree, ef, k),
+so later runs on the same kind of index start from it. Every setting returns
+the same ids (the kernels are exact under all of them); only time differs.
 """
 from __future__ import annotations
 
