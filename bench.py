@@ -259,8 +259,8 @@ def load_peaks():
 
 
 def profile_traffic(kernel, name, ef):
-    """DRAM bytes per query of `kernel` on workload `name` at this ef, from the
-    committed ncu summaries (None when no capture matches)."""
+    """The committed ncu capture of `kernel` on workload `name` at this ef
+    (DRAM bytes per query, L2 sector hit rate), or None."""
     p = os.path.join(ROOT, "profiles", "search_traffic.json")
     try:
         with open(p) as f:
@@ -269,7 +269,7 @@ def profile_traffic(kernel, name, ef):
         return None
     for r in rows:
         if r.get("kernel") == kernel and r.get("workload") == name and r.get("ef") == ef:
-            return float(r["dram_bytes_per_query"])
+            return r
     return None
 
 
@@ -556,8 +556,9 @@ def gpu_arm(args, w, name, rank, world, device):
 
     kernel = {2: "heap_search_kernel", 4: "split_search_kernel", 5: "batch_search_kernel",
               6: "batch_search_kernel (lazy search heap)"}.get(mode)
-    per_query = profile_traffic(kernel, name, chosen) if kernel else None
-    traffic_launch = per_query * nq if per_query is not None else None
+    cap = profile_traffic(kernel, name, chosen) if kernel else None
+    traffic_launch = cap["dram_bytes_per_query"] * nq if cap else None
+    l2_hit = cap.get("l2_hit_rate") if cap else None
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": K,
         "warmup": max(3, args.warmup), "ms_per_step": statistics.mean(step_ms),
@@ -574,7 +575,8 @@ def gpu_arm(args, w, name, rank, world, device):
                    "pops_mean": float(pops.mean()), "evals_mean": float(evals.mean())},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic_launch, "algorithmic_bytes_per_launch": bytes_launch,
+                     "traffic": traffic_launch, "l2_hit_rate": l2_hit,
+                     "algorithmic_bytes_per_launch": bytes_launch,
                      "kernel_ms": statistics.mean(kern_ms),
                      "kernel": {1: "fast_search_kernel + heap_search_kernel (tied queries)",
                                 2: "heap_search_kernel",
