@@ -143,7 +143,8 @@ def _knn_graph(x, deg):
 
 
 @pytest.mark.parametrize("dim,deg,integer", [(128, 32, True), (96, 64, True), (64, 32, False),
-                                             (288, 64, False), (33, 32, True), (130, 32, False)])
+                                             (288, 64, False), (33, 32, True), (130, 32, False),
+                                             (64, 96, True), (48, 128, False)])
 def test_replay_larger_index_uneven_batch(lqg, tmp_path, mode, dim, deg, integer):
     """12k nodes, exact-kNN graph; per-query ef in {1..512} and k in {1, 10, 100}."""
     from oracle.oracle import sq8_quantize
