@@ -140,7 +140,8 @@ LQG_API lqg_status lqg_search(lqg_index* ix, const float* query, uint32_t k,
  *   k, ef    per-query arrays [m] (u32) or NULL, then k0/ef0 apply to all
  *            (ef0 == 0 means the value given to lqg_set_ef). With a per-query
  *            ef array, ef0 must be an upper bound of its values (it sizes the
- *            kernel's pool); per-query k values above kstride are clamped.
+ *            kernel's pool): a per-query ef above ef0 runs at ef0, and 0 runs
+ *            at 1; per-query k values above kstride are clamped.
  *   ids      [m][kstride] u32, compat output as lqg_search writes it
  *   pool_ids [m][pstride] u32, pool_d [m][pstride] f32: the full final pool
  *            in ascending distance (NULL to skip); unused slots LQG_NO_ID/inf
@@ -190,12 +191,16 @@ LQG_API lqg_status lqg_search_exact_device(lqg_index* ix, const float* queries,
  * cudaMalloc/cudaFree could synchronize the device and stall other streams.
  * Same arguments and outputs as lqg_search_exact_device (DEVICE pointers), but
  * the work areas live in a fixed array inside the library (about 1.1 MB per
- * GPU, held until the process exits): ef <= 512, at most 8192 visited nodes
- * and 8192 search-heap entries per query (else LQG_ERR_CAPACITY and that
- * query's ids are LQG_NO_ID). The call waits for `stream` before returning.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture. All calls share the array, so calls
- * that overlap on the GPU (other threads or streams) race: serialize them. */
+ * GPU, held until the process exits). ef (or the per-query ef bound ef0) above
+ * 512 is rejected at the call with LQG_ERR_ARG, as in every search entry
+ * point; a query that needs more than 8192 visited nodes or 8192 search-heap
+ * entries makes the call return LQG_ERR_CAPACITY, with that query's ids set to
+ * LQG_NO_ID and every other query of the batch answered normally. The call
+ * waits for `stream` before returning. The first call on a device looks up
+ * the array's device address and keeps it; make that first call before any
+ * stream capture, and do not reset the device (cudaDeviceReset) after it. All
+ * calls share the array, so calls that overlap on the GPU (other threads or
+ * streams) race: serialize them. */
 LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
                                            int64_t m, const uint32_t* k, uint32_t k0,
                                            const uint32_t* ef, uint32_t ef0,

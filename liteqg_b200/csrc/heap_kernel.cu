@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(256, 2) heap_search_kernel(SearchArgs a, HeapA
         slot = __shfl_sync(kFull, slot, 0);
         if ((int64_t)slot >= mlist) break;
         const int64_t qi = a.qlist ? (int64_t)a.qlist[slot] : (int64_t)slot;
-        uint32_t ef = a.efq ? a.efq[qi] : a.ef0;
+        uint32_t ef = query_ef(a, qi);
         ef = min(max(ef, 1u), hp.rcap - 1u);
         const uint32_t k = min(a.kq ? a.kq[qi] : a.k0, a.kstride);
         const float* q = a.queries + (size_t)qi * dim;

@@ -134,7 +134,7 @@ __device__ __forceinline__ bool replay_result(const SearchArgs& a, const ReplayA
                                               int64_t qi, uint32_t len, const heapops::HeapView rp,
                                               int lane) {
     using namespace heapops;
-    const uint32_t efq = a.efq ? a.efq[qi] : a.ef0;
+    const uint32_t efq = query_ef(a, qi);
     const uint32_t ef = min(max(efq, 1u), ra.efcap);
     const uint32_t k = min(a.kq ? a.kq[qi] : a.k0, a.kstride);
     const uint4* lg = ra.rlog + (size_t)qi * ra.rlog_cap;

@@ -79,6 +79,14 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// ef of query qi: its per-query value when the caller gave an array, clamped
+// to [1, ef0] (ef0 is the batch's bound, checked on the host to be <= 512), so
+// a per-query value above the bound runs at the bound.
+__device__ __forceinline__ uint32_t query_ef(const SearchArgs& a, int64_t qi) {
+    const uint32_t e = a.efq ? a.efq[qi] : a.ef0;
+    return min(max(e, 1u), max(a.ef0, 1u));
+}
+
 __device__ __forceinline__ uint32_t hash_id(uint32_t v, uint32_t bits) {
     return (v * 0x9E3779B1u) >> (32u - bits);
 }

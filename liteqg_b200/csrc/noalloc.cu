@@ -47,12 +47,17 @@ constexpr size_t kNoAllocBytes = kCtlBytes + kVisBytes + kSpBytes + kRpBytes;
 // from cudaGetSymbolAddress on each device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
+static_assert(kNoAllocRCap >= lqg_host::kMaxEf + 2,
+              "the result heap holds ef + 1 entries for every ef the host accepts");
+
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 unsigned char* g_scratch_ptr[kMaxDevices] = {};
 
 // Device address of the array on `device` (current). Looked up once per
-// device, on the first call made on it.
+// device, on the first call made on it, and kept for the life of the process:
+// a device reset (cudaDeviceReset) after that first call is not supported,
+// since the module is reloaded and the kept address goes stale.
 lqg_status scratch_on(int device, unsigned char** out) {
     if (device < 0 || device >= kMaxDevices)
         return lqg_host::fail(LQG_ERR_ARG, "device ordinal out of range for the no-alloc entry");
@@ -78,8 +83,6 @@ extern "C" LQG_API lqg_status lqg_search_exact_noalloc(
     BatchSpec b{queries, m, k, k0, ef, ef0, ids, kstride, pool_ids, pool_d, pstride, stats, st};
     lqg_status s = check_batch(ix, b);
     if (s != LQG_OK) return s;
-    if (b.ef0 > kNoAllocRCap - 8)
-        return fail(LQG_ERR_ARG, "ef above 512 exceeds the no-alloc work area");
     if (m == 0) return LQG_OK;
     DeviceScope ds(ix->device);
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");

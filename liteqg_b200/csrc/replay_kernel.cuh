@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(512) replay_search_kernel(SearchArgs a, Replay
         slot = __shfl_sync(kFull, slot, 0);
         if ((int64_t)slot >= mlist || slot == 0xFFFFFFFFu) break;
         const int64_t qi = a.qlist ? (int64_t)a.qlist[slot] : (int64_t)slot;
-        uint32_t ef = a.efq ? a.efq[qi] : a.ef0;
+        uint32_t ef = query_ef(a, qi);
         ef = min(max(ef, 1u), ra.efcap);  // efcap <= CAP - 32
         const float* q = a.queries + (size_t)qi * dim;
         uint4* rlog = ra.rlog + (size_t)qi * ra.rlog_cap;

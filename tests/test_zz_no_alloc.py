@@ -70,4 +70,67 @@ def test_noalloc_rejects_ef_beyond_its_work_area(golden):
     L = lib()
     r = L.lqg_search_exact_noalloc(ix.handle, q.data_ptr(), q.shape[0], None, 10, None, 600,
                                    ids.data_ptr(), 10, None, None, 0, None, None)
-    assert r == 1 and b"512" in L.lqg_last_error()
+    assert r == LQG_ERR_ARG and b"512" in L.lqg_last_error()
+
+
+LQG_ERR_ARG = 1
+LQG_ERR_CAPACITY = 6
+NOALLOC_VISITED = 8192  # visited nodes per query the fixed work area holds
+
+
+def _random_graph_index(tmp_path, n=20000, dim=48, deg=32, seed=11):
+    """An index file with random neighbour lists: searches at large ef visit
+    most of the graph, so they outgrow the fixed work area."""
+    from oracle.oracle import IndexArrays, sq8_quantize, write_index
+
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, dim), dtype=np.float32)
+    nb = rng.integers(0, n, (n, deg)).astype(np.uint32)
+    codes, params = sq8_quantize(x)
+    ix = IndexArrays(n, dim, deg, 0, x, nb, codes, params)
+    path = str(tmp_path / "random_graph.idx")
+    write_index(path, ix)
+    return path, ix, rng.random((16, dim), dtype=np.float32)
+
+
+def test_noalloc_overflow_is_reported_per_query(tmp_path):
+    """A query that needs more than the fixed work area gets LQG_NO_ID and the
+    call returns LQG_ERR_CAPACITY; every other query of the same batch (a
+    per-query ef array: small and large ef mixed) equals
+    lqg_search_exact_device, whose allocated work area holds them all."""
+    import torch
+
+    import liteqg_b200
+    from liteqg_b200._capi import lib
+    from oracle.oracle import Oracle
+
+    path, arrays, qh = _random_graph_index(tmp_path)
+    m, k = qh.shape[0], 10
+    efq = np.array([512, 16] * (m // 2), dtype=np.uint32)
+    want_or = Oracle(arrays).search(qh, k, efq.astype(np.int32))
+    visited = want_or.evals.astype(np.int64) + 1  # the entry point and every evaluated node
+    assert visited.max() > NOALLOC_VISITED and visited.min() < NOALLOC_VISITED // 2
+    ix = liteqg_b200.Index("QG", "L2", arrays.n, arrays.dim, arrays.deg)
+    ix.load(path)
+    q = torch.from_numpy(qh).cuda()
+    e_dev = torch.from_numpy(efq.view(np.int32)).cuda()
+    stream = torch.cuda.current_stream().cuda_stream
+    L = lib()
+
+    def call(fn):
+        ids = torch.zeros((m, k), dtype=torch.int32, device="cuda")
+        r = fn(ix.handle, q.data_ptr(), m, None, k, e_dev.data_ptr(), 512, ids.data_ptr(), k,
+               None, None, 0, None, stream)
+        return r, ids.cpu().numpy().view(np.uint32)
+
+    r0, want = call(L.lqg_search_exact_device)
+    assert r0 == 0 and L.lqg_stream_status(ix.handle, stream) == 0, L.lqg_last_error()
+    assert np.array_equal(want, want_or.compat)
+    for _ in range(2):
+        r, got = call(L.lqg_search_exact_noalloc)
+        assert r == LQG_ERR_CAPACITY, L.lqg_last_error()
+        over = visited > NOALLOC_VISITED
+        fits = visited <= NOALLOC_VISITED - 64
+        assert (got[over] == 0xFFFFFFFF).all()
+        assert np.array_equal(got[fits], want[fits])
+        assert fits.sum() + over.sum() == m
