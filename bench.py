@@ -134,12 +134,158 @@ def key_of(name, w):
     return f"{name}-{h.hexdigest()[:10]}"
 
 
+def index_path(name, w):
+    return os.path.join(cache_dir(), key_of(name, w) + ".idx")
+
+
+def gt_path(name, w, rank, nq):
+    return os.path.join(cache_dir(), key_of(name, w) + f".gt{rank}-{nq}.npy")
+
+
+def workload_str(name, w, nq, k, ef):
+    """The `config.workload` string; both arms print the same one."""
+    return (f"{name}: N={w['n']} D={w['dim']} deg={w['deg']} EF={w['efb']} "
+            f"(random_edges={w['random_edges']}, path_take={w['path_take']}, "
+            f"far_budget={w['far_budget']}), {nq} queries/GPU, k={k}, ef={ef}")
+
+
+# ------------------------------------------------- the prebuilt bench graph
+# The reference arm runs first on a fresh machine and must neither touch the
+# GPU nor load this package's library, yet it has to search the same index
+# file as the GPU arm. So the GPU builder's graph for the default workload is
+# carried with the repository copy (bench_data/, not committed: neighbour ids
+# packed at ceil(log2 N) bits, the entry point, the FP64 ground truth of the
+# rank-0 queries and the SHA-256 of the whole index file). On the CPU the arm
+# regenerates the base vectors from their seed, SQ8-encodes them with the
+# reference's own encoder (oracle/_ref), writes the reference's file layout
+# and checks the hash; only when that is impossible does it fall back to a
+# child process that runs the GPU builder (recorded in its line).
+DATA_DIR = os.path.join(ROOT, "bench_data")
+
+
+def _id_bits(n):
+    """Bits per packed id: ceil(log2 n) rounded up to a multiple of 4."""
+    return max(4, -(-int(n - 1).bit_length() // 4) * 4)
+
+
+def _pack_ids(ids, bits):
+    """u32 ids < 2^bits -> bytes: two ids per 2*bits/8 bytes, little-endian."""
+    v = np.ascontiguousarray(ids, dtype=np.uint64).reshape(-1)
+    if len(v) % 2:
+        v = np.concatenate([v, np.zeros(1, np.uint64)])
+    word = v[0::2] | (v[1::2] << np.uint64(bits))
+    nb = 2 * bits // 8
+    return word.view(np.uint8).reshape(-1, 8)[:, :nb].tobytes()
+
+
+def _unpack_ids(buf, bits, count):
+    nb = 2 * bits // 8
+    a = np.zeros((len(buf) // nb, 8), np.uint8)
+    a[:, :nb] = np.frombuffer(buf, np.uint8).reshape(-1, nb)
+    word = a.view(np.uint64).reshape(-1)
+    mask = np.uint64((1 << bits) - 1)
+    out = np.empty((len(word), 2), np.uint64)
+    out[:, 0] = word & mask
+    out[:, 1] = (word >> np.uint64(bits)) & mask
+    return out.reshape(-1)[:count].astype(np.uint32)
+
+
+def _sha256(path):
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for blk in iter(lambda: f.read(1 << 24), b""):
+            h.update(blk)
+    return h.hexdigest()
+
+
+def export_shipped(name, w, part, nparts, outdir):
+    """Writes part `part` of `nparts` of the cached index's neighbour lists
+    (packed), plus the metadata and (part 0) the rank-0 ground truth, under
+    outdir; the cached index and ground truth must exist (a GPU-arm run)."""
+    from oracle.oracle import read_index
+
+    path = index_path(name, w)
+    arr = read_index(path, w["n"], w["dim"], w["deg"])
+    bits = _id_bits(w["n"])
+    rows = np.array_split(np.arange(w["n"]), nparts)[part]
+    key = key_of(name, w)
+    os.makedirs(outdir, exist_ok=True)
+    with open(os.path.join(outdir, f"{key}.nbrs{part}of{nparts}.bin"), "wb") as f:
+        f.write(_pack_ids(arr.nbrs[rows[0]:rows[-1] + 1], bits))
+    meta = {"workload": name, "key": key, "n": w["n"], "dim": w["dim"], "deg": w["deg"],
+            "entry": arr.entry, "bits": bits, "nparts": nparts,
+            "sha256": _sha256(path), "builder": BUILDER_VERSION}
+    with open(os.path.join(outdir, f"{key}.meta{part}.json"), "w") as f:
+        json.dump(meta, f)
+    if part == 0:
+        gt = np.load(gt_path(name, w, 0, w["nq"]))
+        np.savez_compressed(os.path.join(outdir, f"{key}.gt0.npz"), gt=gt.astype(np.int32))
+    print(json.dumps(meta), flush=True)
+
+
+def assemble_shipped(name, w, base):
+    """CPU only: the cached index file (and rank-0 ground truth) from
+    bench_data/ and the regenerated base vectors. Returns a note for the
+    JSON line, or None when bench_data/ has no complete, matching copy."""
+    from oracle.oracle import IndexArrays, RefHarness, ref_available, sq8_quantize, write_index
+
+    key = key_of(name, w)
+    try:
+        with open(os.path.join(DATA_DIR, f"{key}.meta0.json")) as f:
+            meta = json.load(f)
+        nparts = meta["nparts"]
+        metas = [meta]
+        for p in range(1, nparts):
+            with open(os.path.join(DATA_DIR, f"{key}.meta{p}.json")) as f:
+                metas.append(json.load(f))
+    except (OSError, ValueError, KeyError):
+        return None
+    if any(m["sha256"] != meta["sha256"] for m in metas):
+        return None
+    rows = np.array_split(np.arange(w["n"]), nparts)
+    nb = np.empty((w["n"], w["deg"]), np.uint32)
+    for p in range(nparts):
+        with open(os.path.join(DATA_DIR, f"{key}.nbrs{p}of{nparts}.bin"), "rb") as f:
+            buf = f.read()
+        cnt = len(rows[p]) * w["deg"]
+        nb[rows[p][0]:rows[p][-1] + 1] = _unpack_ids(buf, meta["bits"], cnt).reshape(-1, w["deg"])
+    if ref_available():
+        codes, params = RefHarness().sq8_quantize(base)
+        enc = "the reference's sq8_quantize (oracle/_ref)"
+    else:
+        codes, params = sq8_quantize(base)
+        enc = "the oracle's SQ8 encoder"
+    path = index_path(name, w)
+    tmp = path + f".tmp{os.getpid()}"
+    write_index(tmp, IndexArrays(w["n"], w["dim"], w["deg"], meta["entry"], base, nb, codes, params))
+    if _sha256(tmp) != meta["sha256"]:
+        os.remove(tmp)
+        return None
+    os.replace(tmp, path)
+    gt = np.load(os.path.join(DATA_DIR, f"{key}.gt0.npz"))["gt"].astype(np.int64)
+    np.save(gt_path(name, w, 0, len(gt)), gt)
+    return (f"index file assembled on the CPU from bench_data/ (GPU builder's graph, "
+            f"{meta['builder']}) with codes from {enc}; SHA-256 matches the built file")
+
+
+def prepare_in_child(name, w):
+    """Fallback of the reference arm: the GPU builder and the GPU ground truth
+    run in a child process, so this process loads neither."""
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--prepare",
+                        "--workload", name], stdout=subprocess.PIPE, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"--prepare failed with {r.returncode}")
+    return "index file built and ground truth computed by a child process (GPU builder)"
+
+
 def get_index_file(name, w, base, device):
     """Builds (GPU builder) or reuses the cached index file."""
     import liteqg_b200
 
-    path = os.path.join(cache_dir(), key_of(name, w) + ".idx")
+    path = index_path(name, w)
     if os.path.exists(path):
+        return path, 0.0
+    if assemble_shipped(name, w, base) is not None:
         return path, 0.0
     ix = liteqg_b200.Index("QG", "L2", w["n"], w["dim"], w["deg"], device=device)
     t = time.perf_counter()
@@ -157,7 +303,7 @@ def ground_truth(name, w, base, queries, device, rank):
     """FP64 brute-force top-100 ids per query (GPU, chunked), cached."""
     import torch
 
-    path = os.path.join(cache_dir(), key_of(name, w) + f".gt{rank}-{len(queries)}.npy")
+    path = gt_path(name, w, rank, len(queries))
     if os.path.exists(path):
         return np.load(path)
     dev = torch.device("cuda", device)
@@ -303,17 +449,19 @@ def time_cpu(fn, queries, budget_s, min_q=256):
 
 # ---------------------------------------------------------------- arms
 def reference_arm(args, w, name):
-    import torch
-
+    """The reference's own search on the host cores. This process loads no GPU
+    code: the index file comes from the cache, from bench_data/ (assembled on
+    the CPU) or, failing both, from a child process running the GPU builder."""
     base = gen_data(w, "base")
     queries = gen_data(w, "query")
-    path, tb = get_index_file(name, w, base, 0)
-    gt = ground_truth(name, w, base, queries, 0, 0)
+    path = index_path(name, w)
+    prep = "index file and ground truth from the cache (built earlier on this machine)"
+    if not (os.path.exists(path) and os.path.exists(gt_path(name, w, 0, len(queries)))):
+        prep = assemble_shipped(name, w, base) or prepare_in_child(name, w)
+    gt = np.load(gt_path(name, w, 0, len(queries)))
     del base
     nthreads = os.cpu_count() or 1
     # same ef rule as the GPU arm, decided with the reference's own pools
-    from oracle.oracle import SENTINEL
-
     chosen, rec = w["efs"][-1], None
     sample = queries[:2000]
     for ef in w["efs"]:
@@ -323,27 +471,37 @@ def reference_arm(args, w, name):
         if rec >= 0.95:
             chosen = ef
             break
-    fn, kind, keep = cpu_reference_search(path, w, queries, w["k"], chosen, nthreads)
-    per = max(256, min(len(queries), 4000))
+    k = w["k"]
+    fn, kind, keep = cpu_reference_search(path, w, queries, k, chosen, nthreads)
     for _ in range(args.warmup):
-        fn(queries[:per])
+        fn(queries)
     times = []
-    for i in range(args.steps):
-        s = (i * per) % max(1, len(queries) - per + 1)
+    for _ in range(args.steps):
         t = time.perf_counter()
-        fn(queries[s:s + per])
+        fn(queries)
         times.append(time.perf_counter() - t)
-    qps = per * len(times) / sum(times)
+    nq = len(queries)
+    qps = nq * len(times) / sum(times)
+    maps = []
+    try:
+        with open("/proc/self/maps") as f:
+            maps = sorted({l.split()[-1] for l in f if l.rstrip().endswith(".so")
+                           and l.split()[-1].startswith(ROOT)})
+    except OSError:
+        pass
     line = {
         "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{name}: reference CPU search, {per} queries per step", "ef": chosen,
-                   "k": w["k"], "recall_at_10_pool": rec, "parallelism": "host threads"},
+        "config": {"workload": workload_str(name, w, nq, k, chosen), "ef": chosen, "k": k,
+                   "recall_at_10_pool": rec, "parallelism": f"{nthreads} host threads, "
+                                                          "one reference search per query"},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": nthreads, "kind": kind,
-                         "sample": f"{per} of {len(queries)} queries per step, k={w['k']}, ef={chosen}"},
+                         "sample": f"all {nq} queries per step, k={k}, ef={chosen}"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "index_prep": prep,
+        "repo_libraries_mapped": [os.path.relpath(m, ROOT) for m in maps],
     }
     print(json.dumps(line), flush=True)
 
@@ -360,9 +518,35 @@ def gpu_arm(args, w, name, rank, world, device):
     base = gen_data(w, "base")
     queries = gen_data(w, "query", rank)
     path, t_build = get_index_file(name, w, base, device)
+    n, dim, deg, nq, k = w["n"], w["dim"], w["deg"], w["nq"], w["k"]
+    if args.profile:
+        # a profiling run holds only the index, the queries and the kernels'
+        # work areas on the device: no ground truth, no ef selection, no
+        # autotuning (ef from --ef, launch shape of --mode, default 6)
+        del base
+        ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
+        ix.load(path)
+        ef = args.ef or w["efs"][0]
+        c = FIXED_TUNING[args.mode or 6]
+        ix.set_tuning(mode=c[0], lanes_per_cand=c[1], visited_bits=c[2], warps_per_block=c[3],
+                      heap_warps=c[4], heap_scap=c[5])
+        dev = torch.device("cuda", device)
+        sh = torch.cuda.current_stream(dev).cuda_stream
+        q_dev = torch.from_numpy(queries).to(dev)
+        ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+        ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=ef, stream=sh)
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_push("lqg_profile")
+        for _ in range(args.profile):
+            ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=ef, stream=sh)
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_pop()
+        ix.stream_status(sh)
+        log(f"[rank {rank}] profiled {args.profile} steps, mode {c[0]}, ef {ef}")
+        ix.close()
+        return
     gt = ground_truth(name, w, base, queries, device, rank)
     log(f"[rank {rank}] data+index+gt ready in {time.perf_counter() - t0:.1f}s (build {t_build:.1f}s)")
-    n, dim, deg, nq, k = w["n"], w["dim"], w["deg"], w["nq"], w["k"]
     ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
     ix.load(path)
     log(f"[rank {rank}] index loaded {time.perf_counter() - t0:.1f}s")
@@ -419,16 +603,6 @@ def gpu_arm(args, w, name, rank, world, device):
         tuned = autotune.tune(ix, queries, chosen, k, path=None, device=device)
         mode = tuned["mode"]
         mode_ms = {str(c): t for t, c in tuned["all"]}
-    if args.profile:
-        torch.cuda.synchronize(dev)
-        torch.cuda.nvtx.range_push("lqg_profile")
-        for _ in range(args.profile):
-            ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=chosen, stream=sh)
-        torch.cuda.synchronize(dev)
-        torch.cuda.nvtx.range_pop()
-        ix.stream_status(sh)
-        log(f"[rank {rank}] profiled {args.profile} steps, mode {mode} {mode_ms}")
-        return
     # algorithmic bytes (per launch): neighbour rows of popped nodes, codes of
     # evaluated nodes (+ the entry), the query; SQ8 params once per CTA
     bytes_launch = float((pops * 4 * deg + (evals + 1) * dim + 4 * dim).sum())
@@ -492,20 +666,11 @@ def gpu_arm(args, w, name, rank, world, device):
     log(f"[rank {rank}] e2e done {time.perf_counter() - t0:.1f}s")
     extra = {}
     if rank == 0 and world == 1:
-        # k = 100 at the same ef
-        ids100 = torch.empty((nq, w["k_extra"]), dtype=torch.int32, device=dev)
-        for _ in range(3):
-            ix.search_device(q_dev.data_ptr(), nq, w["k_extra"], ids100.data_ptr(), w["k_extra"],
-                             ef=max(chosen, w["k_extra"]), stream=sh)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(5):
-            ix.search_device(q_dev.data_ptr(), nq, w["k_extra"], ids100.data_ptr(), w["k_extra"],
-                             ef=max(chosen, w["k_extra"]), stream=sh)
-        b.record(stream)
-        b.synchronize()
-        extra["qps_k100"] = nq * 5 / (a.elapsed_time(b) / 1e3)
-        extra["k100_ef"] = max(chosen, w["k_extra"])
+        # the configuration's grid: k in {10, 100} x ef in the workload's ef
+        # set, each point timed (device-resident, L2 flushed), with its
+        # best-10-of-pool recall, the algorithmic roofline fraction of the
+        # search kernel and its ids against the reference on a sample
+        extra["grid"] = grid_points(ix, w, name, path, queries, q_dev, gt, flush, stream, peak)
         # the same search on a 4x larger batch (these queries and three more
         # query seeds of the workload), L2 flushed: the kernel's throughput
         # with less of the batch's ramp and tail per query
@@ -564,10 +729,7 @@ def gpu_arm(args, w, name, rank, world, device):
         "warmup": max(3, args.warmup), "ms_per_step": statistics.mean(step_ms),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"{name}: N={n} D={dim} deg={deg} EF={w['efb']} "
-                               f"(random_edges={w['random_edges']}, path_take={w['path_take']}, "
-                               f"far_budget={w['far_budget']}), {nq} queries/GPU, "
-                               f"k={k}, ef={chosen}", "ef": chosen, "k": k,
+        "config": {"workload": workload_str(name, w, nq, k, chosen), "ef": chosen, "k": k,
                    "recall_at_10_pool": recall.get(chosen), "recall_by_ef": recall,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                    "tuning": tune, "autotune_ms": mode_ms, "tied_query_share": exact_share,
@@ -600,6 +762,63 @@ def gpu_arm(args, w, name, rank, world, device):
     if rank == 0:
         print(json.dumps(line), flush=True)
     ix.close()
+
+
+def grid_points(ix, w, name, path, queries, q_dev, gt, flush, stream, peak):
+    """k x ef grid of the headline workload (see gpu_arm)."""
+    import torch
+
+    nq, dim, deg = len(queries), w["dim"], w["deg"]
+    sh = stream.cuda_stream
+    dev = q_dev.device
+    nthreads = os.cpu_count() or 1
+    sample = min(1000, nq)
+    out = {}
+    for ef in w["efs"]:
+        st = torch.zeros((nq, 4), dtype=torch.int32, device=dev)
+        idx = torch.empty((nq, 1), dtype=torch.int32, device=dev)
+        ix.search_device(q_dev.data_ptr(), nq, 1, idx.data_ptr(), 1, ef=ef,
+                         stats_ptr=st.data_ptr(), stream=sh, exact=True)
+        stx = st.cpu().numpy().astype(np.int64)
+        bytes_launch = float((stx[:, 0] * 4 * deg + (stx[:, 1] + 1) * dim + 4 * dim).sum())
+        _, (pid, _) = ix.search(queries, 10, ef=ef, return_pool=True)
+        rec = recall_at(pid, gt, 10)
+        for k in (10, w["k_extra"]):
+            ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+
+            def run():
+                ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=ef, stream=sh)
+
+            for _ in range(2):
+                run()
+            ix.stream_status(sh)
+            reps, step_ms, kern_ms = 5, [], []
+            for i in range(reps):
+                flush.fill_(i & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ka, kb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ix.set_kernel_events(ka.cuda_event, kb.cuda_event)
+                a.record(stream)
+                run()
+                b.record(stream)
+                b.synchronize()
+                step_ms.append(a.elapsed_time(b))
+                kern_ms.append(ka.elapsed_time(kb))
+            ix.set_kernel_events(0, 0)
+            ix.stream_status(sh)
+            fn, kind, keep = cpu_reference_search(path, w, queries[:sample], k, ef, nthreads)
+            ref_ids = fn(queries[:sample])
+            got = ids.cpu().numpy().view(np.uint32)[:sample]
+            achieved = bytes_launch / (statistics.mean(kern_ms) / 1e3) / 1e9
+            out[f"k{k}_ef{ef}"] = {
+                "qps": nq / (statistics.mean(step_ms) / 1e3), "ms": statistics.mean(step_ms),
+                "recall_at_10_pool": rec, "roofline_frac": achieved / peak,
+                "achieved_gbs": achieved, "pops_mean": float(stx[:, 0].mean()),
+                "evals_mean": float(stx[:, 1].mean()),
+                "ids_mismatch_vs_reference": int((ref_ids != got).any(1).sum()),
+                "reference_sample": f"first {sample} queries ({kind})"}
+            log(f"[grid] k={k} ef={ef}: {out[f'k{k}_ef{ef}']}")
+    return out
 
 
 def _timed(fn, reps, flush, stream):
@@ -678,8 +897,78 @@ def uneven_arm(args, w, name, device):
         step()
     ix.stream_status(sh)
     K = max(1, min(args.steps, 50))
-    eager_ms = _timed(step, K, flush, stream)
+    eager_ms, kern_ms = [], []
+    for i in range(K):
+        flush.fill_(i & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ka, kb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ix.set_kernel_events(ka.cuda_event, kb.cuda_event)
+        a.record(stream)
+        step()
+        b.record(stream)
+        b.synchronize()
+        eager_ms.append(a.elapsed_time(b))
+        kern_ms.append(ka.elapsed_time(kb))
+    ix.set_kernel_events(0, 0)
+    ix.stream_status(sh)
+    eager_ms = statistics.mean(eager_ms)
     eager_ids = ids.cpu().numpy().copy()
+    # the reference's work per query (pops, evaluations; the exact kernel
+    # counts them exactly) for the algorithmic bytes of the launch
+    stx = torch.zeros((nq, 4), dtype=torch.int32, device=dev)
+    idx = torch.empty((nq, kmax), dtype=torch.int32, device=dev)
+    ix.search_device(q_dev.data_ptr(), nq, 0, idx.data_ptr(), kmax, ef=efmax,
+                     ef_ptr=e_dev.data_ptr(), k_ptr=k_dev.data_ptr(), stats_ptr=stx.data_ptr(),
+                     stream=sh, exact=True)
+    ix.stream_status(sh)
+    stx = stx.cpu().numpy().astype(np.int64)
+    pops, evals = stx[:, 0], stx[:, 1]
+    bytes_launch = float((pops * 4 * deg + (evals + 1) * dim + 4 * dim).sum())
+    achieved = bytes_launch / (statistics.mean(kern_ms) / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    # e2e through the host-buffer C ABI with the per-query k and ef arrays
+    from liteqg_b200._capi import check, lib
+
+    q_pin = torch.from_numpy(queries).pin_memory()
+    ids_pin = torch.empty((nq, kmax), dtype=torch.int32).pin_memory()
+    k_pin = torch.from_numpy(kq.view(np.int32)).pin_memory()
+    e_pin = torch.from_numpy(efq.view(np.int32)).pin_memory()
+    e2e_ms = []
+    for i in range(2 + K):
+        flush.fill_(i & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        check(lib().lqg_search_batch(ix.handle, q_pin.data_ptr(), nq, k_pin.data_ptr(), 0,
+                                     e_pin.data_ptr(), efmax, ids_pin.data_ptr(), kmax, None,
+                                     None, 0, None, sh))
+        b.record(stream)
+        b.synchronize()
+        if i >= 2:
+            e2e_ms.append(a.elapsed_time(b))
+    e2e_qps = nq / (statistics.mean(e2e_ms) / 1e3)
+    col = np.arange(kmax)[None, :] < kq[:, None]
+    e2e_ok = bool((ids_pin.numpy()[col] == eager_ids[col]).all())
+    # CPU baseline: the compiled reference on all host cores, the whole batch
+    # (grouped by (ef, k), its search takes one of each per call)
+    nthreads = os.cpu_count() or 1
+    ref_ids = np.full((nq, kmax), 0xFFFFFFFF, np.uint32)
+    t_cpu, kind = 0.0, None
+    for e in w["ef_choices"]:
+        for kk in w["k_choices"]:
+            sel = np.nonzero((efq == e) & (kq == kk))[0]
+            if len(sel) == 0:
+                continue
+            fn, kind, keep = cpu_reference_search(path, w, queries[sel], int(kk), int(e), nthreads)
+            t = time.perf_counter()
+            out = fn(queries[sel])
+            t_cpu += time.perf_counter() - t
+            ref_ids[sel, :kk] = out
+    got = eager_ids.view(np.uint32)
+    ref_mismatch = int(((ref_ids != got) & col).any(1).sum())
+    cpu = {"value": nq / t_cpu, "unit": "queries/s", "cores": nthreads, "kind": kind,
+           "sample": f"all {nq} queries, each at its own ef and k, {t_cpu:.1f}s wall",
+           "ids_mismatch_vs_gpu": ref_mismatch}
+    log(f"[uneven] cpu {cpu}")
     # the same batch captured in a CUDA graph
     s2 = torch.cuda.Stream(dev)
     s2.wait_stream(stream)
@@ -707,7 +996,20 @@ def uneven_arm(args, w, name, device):
                    "mode": best[1], "lanes_per_cand": best[2],
                    "l2": "flushed between steps (256 MiB write)"},
         "graph_qps": nq / (graph_ms / 1e3), "graph_ids_equal": graph_ok,
-        "gpu_launches": {1: 3, 2: 2, 4: 2}.get(best[1], 3) * K,
+        "gpu_launches": (5 + {1: 3, 2: 2, 3: 3, 4: 2, 5: 2, 6: 2}.get(best[1], 3)) * K,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": bytes_launch,
+                     "kernel_ms": statistics.mean(kern_ms),
+                     "kernel": {1: "fast_search_kernel + heap_search_kernel (tied queries)",
+                                2: "heap_search_kernel", 4: "split_search_kernel",
+                                5: "batch_search_kernel",
+                                6: "batch_search_kernel (lazy search heap)"}.get(best[1])},
+        "e2e": {"value": e2e_qps, "unit": "queries/s",
+                "h2d_bytes_per_step": int(nq * dim * 4 + 8 * nq),
+                "d2h_bytes_per_step": int(nq * kmax * 4), "ids_equal": e2e_ok},
+        "cpu_baseline": cpu,
+        "pops_mean": float(pops.mean()), "evals_mean": float(evals.mean()),
     }
     print(json.dumps(line), flush=True)
 
@@ -779,13 +1081,27 @@ def serving_arm(args, w, name, device):
             efs = rng.choice(w["ef_choices"], m).astype(np.uint32)
             srv.reset_stats()
             t = time.perf_counter()
-            _, lat = srv.replay(queries[:m], ks, efs, arrivals)
+            sids, lat = srv.replay(queries[:m], ks, efs, arrivals)
             wall = time.perf_counter() - t
             st = srv.stats()
+            # ids of a sample of the served requests against the reference's
+            # own search of each alone (its k and ef)
+            samp = rng.choice(m, min(m, 1000), replace=False)
+            mism = 0
+            for e in w["ef_choices"]:
+                for kk in w["k_choices"]:
+                    sel = samp[(efs[samp] == e) & (ks[samp] == kk)]
+                    if len(sel) == 0:
+                        continue
+                    fn, kind, keep = cpu_reference_search(path, w, queries[sel], int(kk), int(e),
+                                                          os.cpu_count() or 1)
+                    mism += int((fn(queries[sel]) != sids[sel, :kk]).any(1).sum())
             rows.append({"offered_qps": rate, "requests": m, "achieved_qps": m / wall,
                          "p50_ms": float(np.percentile(lat, 50)) / 1e3,
                          "p99_ms": float(np.percentile(lat, 99)) / 1e3,
-                         "mean_batch": st["mean_batch"]})
+                         "mean_batch": st["mean_batch"],
+                         "ids_mismatch_vs_reference": mism,
+                         "reference_sample": f"{len(samp)} served requests ({kind})"})
             log(f"[serving] {rows[-1]}")
     # plain path: one query per call
     lat = []
@@ -932,10 +1248,28 @@ def main():
                     help="use this kernel mode (see lqg_tuning) instead of the autotuner's choice")
     ap.add_argument("--build-only", action="store_true",
                     help="build the workload's index (no cache), print the build report, exit")
+    ap.add_argument("--ef", type=int, default=0, help="--profile: the ef to search with")
+    ap.add_argument("--prepare", action="store_true",
+                    help="build (or assemble) the workload's cached index file and rank-0 "
+                         "ground truth, then exit")
+    ap.add_argument("--export-shipped", default="",
+                    help="PART/NPARTS:DIR - write that part of the cached index's packed "
+                         "graph (and metadata, ground truth) under DIR, then exit")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.build_only:
         build_only(w, args.workload, int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    if args.prepare:
+        base = gen_data(w, "base")
+        path, tb = get_index_file(args.workload, w, base, 0)
+        ground_truth(args.workload, w, base, gen_data(w, "query"), 0, 0)
+        print(json.dumps({"prepared": path, "build_s": tb}), flush=True)
+        return
+    if args.export_shipped:
+        pn, outdir = args.export_shipped.split(":", 1)
+        part, nparts = (int(x) for x in pn.split("/"))
+        export_shipped(args.workload, w, part, nparts, outdir)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

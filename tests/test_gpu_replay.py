@@ -252,3 +252,44 @@ def test_repeated_ids_across_list_words(lqg, tmp_path, fix_mode):
         assert np.array_equal(ids, want.compat), ef
         assert np.array_equal(pd, want.pool_d), ef
         assert np.array_equal(st[:, 0], want.pops), ef
+
+
+@pytest.mark.parametrize("hd_mode", [2, 4, 5, 6])
+def test_high_dimension_degree_64_uneven_batch(lqg, tmp_path, hd_mode):
+    """The uneven high-dimension workload's shape at 12k nodes: D = 960
+    (960-byte code rows, the long code-load window), degree 64, a float
+    Gaussian mixture (centres N(0, 1), sigma 0.3), an exact-kNN graph, and one
+    batch with per-query ef up to 512 and k in {1, 10, 100}: ids, pops and
+    FP32 pools equal the oracle's in the heap kernel (mode 2, the tuner's
+    choice there), the split kernel (4) and the batch kernels (5, 6)."""
+    from oracle.oracle import sq8_quantize
+
+    rng = np.random.default_rng(960)
+    n, dim, deg = 12000, 960, 64
+    cent = rng.normal(0.0, 1.0, (8, dim))  # 1,500 nodes per cluster: every pool fills
+    gen = lambda m: (cent[rng.integers(0, 8, m)] + rng.normal(0.0, 0.3, (m, dim))).astype(np.float32)
+    x = gen(n)
+    codes, params = sq8_quantize(x)
+    arr = IndexArrays(n, dim, deg, int(rng.integers(0, n)), x, _knn_graph(x, deg), codes, params)
+    path = str(tmp_path / "hd.idx")
+    write_index(path, arr)
+    ix = lqg.Index("QG", "L2", n, dim, deg)
+    ix.load(path)
+    ix.set_tuning(mode=hd_mode, lanes_per_cand=2, heap_scap=512)
+    o = Oracle(arr)
+    q = gen(300)
+    efq = rng.choice([32, 64, 128, 256, 512], size=len(q)).astype(np.uint32)
+    kq = rng.choice([1, 10, 100], size=len(q)).astype(np.uint32)
+    ids, st = _device(ix, q, 512, 100, kq=kq, efq=efq)
+    want = o.search(q, kq.astype(np.int32), efq.astype(np.int32))
+    for i in range(len(q)):
+        k = int(kq[i])
+        assert np.array_equal(ids[i, :k], want.compat[i, :k]), (i, efq[i], k)
+    assert np.array_equal(st[:, 0], want.pops)
+    for ef, k in ((64, 10), (512, 100)):
+        w = o.search(q[:100], k, ef)
+        got, (pid, pd), st2 = ix.search(q[:100], k, ef=ef, return_pool=True, return_stats=True)
+        assert np.array_equal(got, w.compat), (ef, k)
+        assert np.array_equal(pd, w.pool_d), (ef, k)
+        assert np.array_equal(pid, w.pool_ids), (ef, k)
+        assert np.array_equal(st2[:, 0], w.pops), (ef, k)
