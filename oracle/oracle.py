@@ -249,3 +249,230 @@ class _RefIndex:
             self.close()
         except Exception:
             pass
+
+
+# ---- upstream FastScan / RaBitQ path --------------------------------------
+
+class _FsoIndex(C.Structure):
+    _fields_ = [
+        ("vectors", C.c_void_p),
+        ("nbrs", C.c_void_p),
+        ("codes", C.c_void_p),
+        ("factors", C.c_void_p),
+        ("diag", C.c_void_p),
+        ("n", C.c_uint64),
+        ("dim", C.c_uint32),
+        ("P", C.c_uint32),
+        ("deg", C.c_uint32),
+        ("entry", C.c_uint32),
+    ]
+
+
+def padded_dim(dim: int) -> int:
+    p = 1
+    while p < dim:
+        p <<= 1
+    return p
+
+
+@dataclass
+class FsArrays:
+    """A FastScan index: graph + raw vectors + per-node neighbour codes/factors.
+    codes [n][deg][P/8] (byte b: 4-dimension groups 2b low nibble, 2b+1 high
+    nibble, the group's first dimension on the nibble's bit 3); factors
+    [n][3][deg] (triple_x, factor_dq, factor_vq); diag [P]."""
+    n: int
+    dim: int
+    deg: int
+    entry: int
+    vectors: np.ndarray
+    nbrs: np.ndarray
+    codes: np.ndarray
+    factors: np.ndarray
+    diag: np.ndarray
+
+    @property
+    def P(self) -> int:
+        return padded_dim(self.dim)
+
+
+class FsOracle:
+    """CPU restatement of the upstream sorted-buffer FastScan search (fs_oracle.c)."""
+
+    def __init__(self, fs: FsArrays | None = None):
+        self.lib = C.CDLL(ORACLE_SO)
+        self.lib.fso_l2.restype = C.c_float
+        self.lib.fso_search_batch.restype = C.c_int
+        self.fs = fs
+        if fs is not None:
+            self._keep = (np.ascontiguousarray(fs.vectors, np.float32),
+                          np.ascontiguousarray(fs.nbrs, np.uint32),
+                          np.ascontiguousarray(fs.codes, np.uint8),
+                          np.ascontiguousarray(fs.factors, np.float32),
+                          np.ascontiguousarray(fs.diag, np.float32))
+            self.c = _FsoIndex(*[_ptr(a) for a in self._keep], fs.n, fs.dim, fs.P, fs.deg,
+                               fs.entry)
+
+    def rotate(self, x, diag):
+        x = np.ascontiguousarray(np.atleast_2d(x), np.float32)
+        diag = np.ascontiguousarray(diag, np.float32)
+        P = len(diag)
+        out = np.empty((x.shape[0], P), np.float32)
+        for i in range(x.shape[0]):
+            self.lib.fso_rotate(_ptr(x[i]), x.shape[1], P, _ptr(diag), _ptr(out[i]))
+        return out
+
+    def query_prepare(self, rot):
+        rot = np.ascontiguousarray(rot, np.float32)
+        P = len(rot)
+        lut = np.empty(P * 4, np.uint8)
+        w, lo, sq = C.c_float(), C.c_float(), C.c_int32()
+        self.lib.fso_query_prepare(_ptr(rot), P, _ptr(lut), C.byref(w), C.byref(lo), C.byref(sq))
+        return lut, w.value, lo.value, sq.value
+
+    def rabitq(self, rot_nb, rot_c):
+        rot_nb = np.ascontiguousarray(rot_nb, np.float32)
+        rot_c = np.ascontiguousarray(rot_c, np.float32)
+        deg, P = rot_nb.shape
+        bits = np.empty((deg, P // 8), np.uint8)
+        fac = np.empty((3, deg), np.float32)
+        self.lib.fso_rabitq(_ptr(rot_nb), _ptr(rot_c), deg, P, _ptr(bits), _ptr(fac))
+        return bits, fac
+
+    def pack(self, bits):
+        bits = np.ascontiguousarray(bits, np.uint8)
+        ncode, rowb = bits.shape
+        out = np.empty(ncode * rowb, np.uint8)
+        self.lib.fso_pack_codes(_ptr(bits), ncode, rowb * 8, _ptr(out))
+        return out
+
+    def unpack(self, packed, ncode, P):
+        packed = np.ascontiguousarray(packed, np.uint8)
+        bits = np.empty((ncode, P // 8), np.uint8)
+        self.lib.fso_unpack_codes(_ptr(packed), ncode, P, _ptr(bits))
+        return bits
+
+    def accumulate(self, bits, lut):
+        bits = np.ascontiguousarray(bits, np.uint8)
+        lut = np.ascontiguousarray(lut, np.uint8)
+        ncode, rowb = bits.shape
+        res = np.empty(ncode, np.uint16)
+        self.lib.fso_accumulate(_ptr(bits), ncode, rowb * 8, _ptr(lut), _ptr(res))
+        return res
+
+    def estimate(self, res, sumq, width, lower, sqr_y, factors):
+        res = np.ascontiguousarray(res, np.uint16)
+        factors = np.ascontiguousarray(factors, np.float32)
+        out = np.empty(len(res), np.float32)
+        self.lib.fso_estimate(_ptr(res), len(res), C.c_int32(sumq), C.c_float(width),
+                              C.c_float(lower), C.c_float(sqr_y), _ptr(factors), _ptr(out))
+        return out
+
+    def l2(self, a, b):
+        a = np.ascontiguousarray(a, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        return float(self.lib.fso_l2(_ptr(a), _ptr(b), len(a)))
+
+    def search(self, q, k, ef, nthreads: int = 0):
+        """ids [m][max k] (the reference's copy-out; never-filled slots 0) and
+        stats [m][4]: buffer pops, exact evaluations of popped nodes, exact
+        evaluations in update_results, result count."""
+        q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+        m = q.shape[0]
+        ka = np.broadcast_to(np.asarray(k, np.int32), (m,)).copy()
+        ea = np.broadcast_to(np.asarray(ef, np.int32), (m,)).copy()
+        kmax = int(ka.max())
+        ids = np.zeros((m, kmax), np.uint32)
+        st = np.zeros((m, 4), np.int32)
+        r = self.lib.fso_search_batch(C.byref(self.c), _ptr(q), C.c_int64(m), _ptr(ka), _ptr(ea),
+                                      _ptr(ids), kmax, _ptr(st), nthreads)
+        if r != 0:
+            raise MemoryError("FastScan oracle search failed")
+        return ids, st
+
+
+def fs_encode(vectors, nbrs, diag, oracle: FsOracle | None = None):
+    """Per-node neighbour codes and factors of a graph (oracle restatement)."""
+    o = oracle or FsOracle()
+    vectors = np.ascontiguousarray(vectors, np.float32)
+    n, dim = vectors.shape
+    deg = nbrs.shape[1]
+    P = len(diag)
+    rot = o.rotate(vectors, diag)
+    codes = np.empty((n, deg, P // 8), np.uint8)
+    fac = np.empty((n, 3, deg), np.float32)
+    for i in range(n):
+        codes[i], fac[i] = o.rabitq(rot[nbrs[i]], rot[i])
+    return codes, fac
+
+
+class RefFastScan:
+    """The reference's own upstream FastScan/RaBitQ functions (oracle/_ref)."""
+
+    def __init__(self):
+        self.lib = C.CDLL(REF_SO)
+        self.lib.ref_fs_open.restype = C.c_void_p
+        self.lib.ref_fs_open.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32] + \
+            [C.c_void_p] * 5
+        self.lib.ref_fs_close.argtypes = [C.c_void_p]
+        self.lib.ref_fs_search.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                                           C.c_void_p, C.c_int]
+        self.lib.ref_fs_rotate.argtypes = [C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64,
+                                           C.c_void_p]
+        self.lib.ref_fs_query_prepare.argtypes = [C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        self.lib.ref_fs_rabitq.argtypes = [C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]
+        self.lib.ref_fs_scan.argtypes = [C.c_uint64, C.c_uint64, C.c_void_p, C.c_float,
+                                         C.c_float, C.c_float, C.c_int32, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]
+
+    def rotate(self, x, diag):
+        x = np.ascontiguousarray(np.atleast_2d(x), np.float32)
+        diag = np.ascontiguousarray(diag, np.float32)
+        out = np.empty((x.shape[0], len(diag)), np.float32)
+        self.lib.ref_fs_rotate(x.shape[1], _ptr(diag), _ptr(x), x.shape[0], _ptr(out))
+        return out
+
+    def query_prepare(self, q, diag, deg=32):
+        q = np.ascontiguousarray(q, np.float32)
+        diag = np.ascontiguousarray(diag, np.float32)
+        lut = np.empty(len(diag) * 4, np.uint8)
+        w, lo, sq = C.c_float(), C.c_float(), C.c_int32()
+        self.lib.ref_fs_query_prepare(len(q), deg, _ptr(diag), _ptr(q), _ptr(lut), C.byref(w),
+                                      C.byref(lo), C.byref(sq))
+        return lut, w.value, lo.value, sq.value
+
+    def rabitq(self, rot_nb, rot_c):
+        rot_nb = np.ascontiguousarray(rot_nb, np.float32)
+        rot_c = np.ascontiguousarray(rot_c, np.float32)
+        deg, P = rot_nb.shape
+        packed = np.empty(deg * P // 8, np.uint8)
+        fac = np.empty((3, deg), np.float32)
+        self.lib.ref_fs_rabitq(P, deg, _ptr(rot_nb), _ptr(rot_c), _ptr(packed), _ptr(fac))
+        return packed, fac
+
+    def scan(self, lut, sqr_y, lower, width, sumq, packed, factors, deg):
+        lut = np.ascontiguousarray(lut, np.uint8)
+        packed = np.ascontiguousarray(packed, np.uint8)
+        factors = np.ascontiguousarray(factors, np.float32)
+        out = np.empty(deg, np.float32)
+        self.lib.ref_fs_scan(len(lut) // 4, deg, _ptr(lut), sqr_y, lower, width, sumq,
+                             _ptr(packed), _ptr(factors), _ptr(out))
+        return out
+
+    def search(self, fs: FsArrays, q, k, ef, nthreads=0):
+        o = FsOracle()
+        P = fs.P
+        packed = np.stack([o.pack(fs.codes[i]) for i in range(fs.n)])
+        keep = (np.ascontiguousarray(fs.vectors, np.float32), np.ascontiguousarray(fs.nbrs, np.uint32),
+                packed, np.ascontiguousarray(fs.factors, np.float32),
+                np.ascontiguousarray(fs.diag, np.float32))
+        h = self.lib.ref_fs_open(fs.n, fs.dim, fs.deg, fs.entry, *[_ptr(a) for a in keep])
+        try:
+            q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+            out = np.zeros((q.shape[0], k), np.uint32)
+            self.lib.ref_fs_search(h, _ptr(q), q.shape[0], k, ef, _ptr(out), nthreads)
+        finally:
+            self.lib.ref_fs_close(h)
+        return out
