@@ -797,6 +797,8 @@ def grid_points(ix, w, name, path, queries, q_dev, gt, flush, stream, peak):
                 flush.fill_(i & 0xFF)
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 ka, kb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ka.record(stream)  # materialise the handles the library records into
+                kb.record(stream)
                 ix.set_kernel_events(ka.cuda_event, kb.cuda_event)
                 a.record(stream)
                 run()
@@ -902,6 +904,8 @@ def uneven_arm(args, w, name, device):
         flush.fill_(i & 0xFF)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ka, kb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ka.record(stream)  # materialise the handles the library records into
+        kb.record(stream)
         ix.set_kernel_events(ka.cuda_event, kb.cuda_event)
         a.record(stream)
         step()

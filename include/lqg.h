@@ -322,6 +322,64 @@ LQG_API lqg_status lqg_device_arrays(const lqg_index* ix, const uint32_t** nbrs,
                              const uint8_t** codes, const float** params,
                              uint32_t* code_stride);
 
+/* ---- FastScan / RaBitQ search (upstream SymphonyQG) ----------------------
+ * The query path this fork still carries but no longer calls:
+ * QuantizedGraph::search_qg (symqglib/qg/qg.hpp:252-287, the call commented
+ * out at qg.hpp:241) with scan_neighbors (:348-393), the sorted SearchBuffer
+ * and ResultBuffer (utils/buffer.hpp:10-119) and update_results (:395-418).
+ * It needs per-node RaBitQ codes and factors of the node's neighbours
+ * (quantization/rabitq.hpp:23-108), which the fork's builder never writes
+ * (update_qg, qg.hpp:475-502, was truncated): lqg_fs_build writes them.
+ * P = 2^ceil(log2 D). In the index file they follow the reference's bytes as
+ * a section ("LQGFS1", P, degree_bound, D, the rotation's diagonal[P], then
+ * per node deg*P/8 code bytes in upstream's FastScan block layout and
+ * triple_x/factor_dq/factor_vq[deg]); lqg_load reads it when present and
+ * lqg_save writes it. The reference's loader reads its own bytes and stops
+ * there, so such a file still loads in the reference. */
+
+/* Encodes the current graph: a seeded +-1/sqrt(P) rotation diagonal (the
+ * reference's FHTRotator seeds from std::random_device and does not save it,
+ * utils/rotator.hpp:31-47), the FHT of every vector, and for every node and
+ * neighbour the sign bits of the rotated residual and its three factors
+ * (norms and inner products reduced in FP64). A neighbour equal to its node
+ * gets zero factors (the reference would divide 0 by 0). No reference
+ * counterpart runs: upstream's QuantizedGraph::update_qg. */
+LQG_API lqg_status lqg_fs_build(lqg_index* ix, uint64_t seed);
+
+/* The section's arrays (host buffers): diag[P]; packed[N][deg*P/8] in
+ * upstream's FastScan block layout (quantization/fastscan_impl.hpp:63-123);
+ * factors[N][3][deg]. set replaces them (for codes made elsewhere, e.g. by
+ * the reference's own rabitq_codes); get copies them out (any pointer may be
+ * NULL; padded_dim receives P). */
+LQG_API lqg_status lqg_fs_set_arrays(lqg_index* ix, const float* diag, const uint8_t* packed,
+                                     const float* factors);
+LQG_API lqg_status lqg_fs_get_arrays(const lqg_index* ix, uint32_t* padded_dim, float* diag,
+                                     uint8_t* packed, float* factors);
+
+/* search_qg for m queries. DEVICE pointers, asynchronous on `stream`.
+ * k/ef per query or k0/ef0 for all (ef0 == 0: the set_ef value; with a
+ * per-query ef array ef0 bounds it); ef in [1, 512], kstride <= 1024.
+ * ids[m][kstride]: the k ids the reference copies out, ascending exact
+ * distance; slots its zero-initialised result buffer never fills hold 0, as
+ * in the reference. stats[m][4] (NULL to skip): search-buffer pops, exact
+ * distances of popped nodes, exact distances in update_results, results. */
+LQG_API lqg_status lqg_fs_search_batch_device(lqg_index* ix, const float* queries, int64_t m,
+                                              const uint32_t* k, uint32_t k0, const uint32_t* ef,
+                                              uint32_t ef0, uint32_t* ids, uint32_t kstride,
+                                              uint32_t* stats, void* stream);
+/* Waits for `stream`; LQG_OK, or the first device-side failure of the last
+ * FastScan batch (a non-finite distance: that query's ids are LQG_NO_ID). */
+LQG_API lqg_status lqg_fs_stream_status(lqg_index* ix, void* stream);
+/* The same with HOST buffers (copies in, searches, copies out, synchronizes). */
+LQG_API lqg_status lqg_fs_search_batch(lqg_index* ix, const float* queries, int64_t m,
+                                       const uint32_t* k, uint32_t k0, const uint32_t* ef,
+                                       uint32_t ef0, uint32_t* ids, uint32_t kstride,
+                                       uint32_t* stats, void* stream);
+/* One query, host buffers (upstream's Index.search: qg.hpp:235-243 with
+ * search_qg); results[k]. */
+LQG_API lqg_status lqg_fs_search(lqg_index* ix, const float* query, uint32_t k,
+                                 uint32_t* results);
+
 #ifdef __cplusplus
 }
 #endif

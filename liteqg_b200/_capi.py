@@ -56,6 +56,15 @@ SIGNATURES = {
     "lqg_get_tuning": (C.c_int, [_vp, _vp]),
     "lqg_info": (C.c_int, [_vp, C.POINTER(C.c_uint64), _u32p, _u32p, _u32p, _u32p]),
     "lqg_device_arrays": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), _u32p]),
+    "lqg_fs_build": (C.c_int, [_vp, C.c_uint64]),
+    "lqg_fs_set_arrays": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "lqg_fs_get_arrays": (C.c_int, [_vp, _u32p, _vp, _vp, _vp]),
+    "lqg_fs_search_batch_device": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp,
+                                             C.c_uint32, _vp, C.c_uint32, _vp, _vp]),
+    "lqg_fs_stream_status": (C.c_int, [_vp, _vp]),
+    "lqg_fs_search_batch": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
+                                      _vp, C.c_uint32, _vp, _vp]),
+    "lqg_fs_search": (C.c_int, [_vp, _vp, C.c_uint32, _vp]),
 }
 
 

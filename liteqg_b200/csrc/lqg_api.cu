@@ -530,12 +530,15 @@ lqg_status lqg_load(lqg_index* ix, const char* path) {
     const long long size = std::ftell(f);
     std::fseek(f, 0, SEEK_SET);
     const uint64_t want = file_bytes(ix->n, ix->dim, ix->deg);
-    if (size < 0 || (uint64_t)size != want) {
+    // the reference's bytes, optionally followed by a FastScan section
+    const bool with_fs = size >= 0 && (uint64_t)size == want + fs_file_bytes(ix);
+    if (size < 0 || ((uint64_t)size != want && !with_fs)) {
         std::fclose(f);
         return fail(LQG_ERR_IO, std::string(path) + ": " + std::to_string(size) +
                                     " bytes, expected " + std::to_string(want) +
                                     " for the index's N, dimension and degree_bound");
     }
+    ix->fs.release();
     try {
         ix->vectors.resize(ix->n * ix->dim);
         ix->nbrs.resize(ix->n * ix->deg);
@@ -560,11 +563,15 @@ lqg_status lqg_load(lqg_index* ix, const char* path) {
     }
     ok = ok && std::fread(ix->codes.data(), 1, ix->codes.size(), f) == ix->codes.size();
     ok = ok && std::fread(ix->params.data(), 4, ix->params.size(), f) == ix->params.size();
-    std::fclose(f);
-    if (!ok) return fail(LQG_ERR_IO, std::string("short read from ") + path);
+    if (!ok) {
+        std::fclose(f);
+        return fail(LQG_ERR_IO, std::string("short read from ") + path);
+    }
     lqg_status s = validate_content(ix);
-    if (s != LQG_OK) return s;
-    return upload(ix);
+    if (s == LQG_OK) s = upload(ix);
+    if (s == LQG_OK && with_fs) s = fs_read(ix, f);
+    std::fclose(f);
+    return s;
 }
 
 lqg_status lqg_save(const lqg_index* ix, const char* path) {
@@ -587,6 +594,7 @@ lqg_status lqg_save(const lqg_index* ix, const char* path) {
     }
     ok = ok && std::fwrite(ix->codes.data(), 1, ix->codes.size(), f) == ix->codes.size();
     ok = ok && std::fwrite(ix->params.data(), 4, ix->params.size(), f) == ix->params.size();
+    if (ok && ix->fs.ready) ok = fs_write(ix, f) == LQG_OK;
     ok = (std::fclose(f) == 0) && ok;
     return ok ? LQG_OK : fail(LQG_ERR_IO, std::string("write to ") + path + " failed");
 }
@@ -604,6 +612,7 @@ lqg_status lqg_set_arrays(lqg_index* ix, uint32_t entry, const float* vectors,
         return fail(LQG_ERR_NOMEM, "host allocation failed");
     }
     ix->entry = entry;
+    ix->fs.release();  // the graph changed: its FastScan section is stale
     lqg_status s = validate_content(ix);
     if (s != LQG_OK) return s;
     return upload(ix);
@@ -952,6 +961,7 @@ lqg_status lqg_build_ex(lqg_index* ix, const float* data, uint32_t ef_build, uin
     ix->entry = (uint32_t)(best & 0xFFFFFFFFull);
     LQG_BCUDA(lqg::launch_random_fill(ix->d_nbrs, nullptr, n, deg, seed, st), "random graph");
     ix->has_data = true;
+    ix->fs.release();  // a new graph: any FastScan section is stale
 
     for (uint32_t it = 0; it < num_iter; ++it) {
         for (uint64_t c0 = 0; c0 < n; c0 += chunk) {

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -156,6 +157,27 @@ lqg_status ensure_exact(Workspace& w, int blocks, int warps_per_block);
 lqg_status reset_ctl(Workspace& w, cudaStream_t st);
 lqg_status read_status(Workspace& w, cudaStream_t st);
 
+// FastScan section of an index (fastscan.cu): per node, the RaBitQ codes and
+// factors of its neighbours around the node, and the rotation's diagonal.
+// Host copies in the file's layout (codes in upstream's FastScan blocks),
+// device rows in the search kernel's.
+struct FsSection {
+    bool ready = false;
+    uint32_t P = 0;                 // padded dimension
+    std::vector<float> diag;        // [P]
+    std::vector<uint8_t> packed;    // [n][deg * P / 8]
+    std::vector<float> factors;     // [n][3][deg]
+    unsigned char* d_rows = nullptr;
+    float* d_diag = nullptr;
+    uint64_t row_bytes = 0;
+    uint32_t off_codes = 0, off_fac = 0, off_ids = 0;
+    void release() {
+        dfree(d_rows);
+        dfree(d_diag);
+        ready = false;
+    }
+};
+
 }  // namespace lqg_host
 
 struct lqg_index {
@@ -177,6 +199,7 @@ struct lqg_index {
     float* d_params = nullptr;
 
     lqg_host::Workspace ws;  // the default work area (one batch at a time)
+    lqg_host::FsSection fs;  // FastScan section (empty until built or loaded)
 
     cudaStream_t own_stream = nullptr;
     // default: the batch kernel with the lazy search heap (mode 6), the
@@ -192,6 +215,7 @@ struct lqg_index {
         lqg_host::dfree(d_codes);
         lqg_host::dfree(d_params);
         ws.release();
+        fs.release();
         if (own_stream) cudaStreamDestroy(own_stream);
         cudaSetDevice(prev);
     }
@@ -209,4 +233,9 @@ lqg_status search_host(lqg_index* ix, Workspace& w, const float* queries, int64_
                        const uint32_t* k, uint32_t k0, const uint32_t* ef, uint32_t efb,
                        uint32_t* ids, uint32_t kstride, uint32_t* pool_ids, float* pool_d,
                        uint32_t pstride, uint32_t* stats, cudaStream_t st);
+// FastScan section in the index file (fastscan.cu): appended after the
+// reference's bytes, which the reference's loader reads and stops at.
+uint64_t fs_file_bytes(const lqg_index* ix);
+lqg_status fs_read(lqg_index* ix, FILE* f);
+lqg_status fs_write(const lqg_index* ix, FILE* f);
 }  // namespace lqg_host

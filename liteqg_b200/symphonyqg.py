@@ -212,6 +212,78 @@ class Index:
         check(lib().lqg_get_tuning(self.handle, C.byref(t)))
         return {f: int(getattr(t, f)) for f, _ in Tuning._fields_}
 
+    # -- FastScan / RaBitQ search (upstream search_qg) -------------------
+    def fastscan_build(self, seed: int = 0) -> None:
+        """Writes the FastScan section for the current graph: a seeded rotation,
+        and per node the RaBitQ codes and factors of its neighbours."""
+        check(lib().lqg_fs_build(self.handle, int(seed)))
+
+    def fastscan_arrays(self):
+        """(diag[P], packed[N][deg*P/8] in upstream's FastScan block layout,
+        factors[N][3][deg])."""
+        P = C.c_uint32()
+        check(lib().lqg_fs_get_arrays(self.handle, C.byref(P), None, None, None))
+        n, g = self.num_elements, self.degree_bound
+        diag = np.empty(P.value, np.float32)
+        packed = np.empty((n, g * P.value // 8), np.uint8)
+        fac = np.empty((n, 3, g), np.float32)
+        check(lib().lqg_fs_get_arrays(self.handle, None, _p(diag), _p(packed), _p(fac)))
+        return diag, packed, fac
+
+    def set_fastscan_arrays(self, diag, packed, factors) -> None:
+        d = _as_f32(diag)
+        pk = np.ascontiguousarray(packed, dtype=np.uint8)
+        fc = _as_f32(factors)
+        P = 1
+        while P < self.dimension:
+            P <<= 1
+        n, g = self.num_elements, self.degree_bound
+        if d.shape != (P,) or pk.size != n * g * P // 8 or fc.size != n * 3 * g:
+            raise ValueError("FastScan array shapes do not match the index")
+        check(lib().lqg_fs_set_arrays(self.handle, _p(d), _p(pk), _p(fc)))
+
+    def search_fastscan(self, query, k: int, ef=None, return_stats: bool = False):
+        """Upstream's search_qg: the k nearest popped nodes by exact distance.
+        ``ef`` (int or per-row array) overrides set_ef. A 1-D query returns
+        uint32[k]; a 2-D block uint32[M, k]. Slots the reference's result
+        buffer never fills hold 0, as in the reference."""
+        q = _as_f32(query)
+        one = q.ndim == 1
+        if one:
+            q = q.reshape(1, -1)
+        if q.ndim != 2 or q.shape[1] != self.dimension:
+            raise ValueError("query must be [D] or [M, D] with D the index dimension")
+        k = int(k)
+        if k < 1:
+            raise ValueError("k must be >= 1")
+        m = q.shape[0]
+        ef_arr, ef0 = None, 0
+        if ef is not None:
+            if np.ndim(ef) == 0:
+                ef0 = int(ef)
+            else:
+                ef_arr = np.ascontiguousarray(ef, dtype=np.uint32)
+                if ef_arr.shape != (m,):
+                    raise ValueError("per-query ef must have one value per query row")
+                ef0 = int(ef_arr.max()) if m else 1
+        ids = np.full((m, k), LQG_NO_ID, dtype=np.uint32)
+        stats = np.zeros((m, 4), dtype=np.uint32) if return_stats else None
+        if m:
+            check(lib().lqg_fs_search_batch(self.handle, _p(q), m, None, k, _p(ef_arr), ef0,
+                                            _p(ids), k, _p(stats), None))
+        res = ids[0] if one else ids
+        return (res, stats) if return_stats else res
+
+    def search_fastscan_device(self, q_ptr: int, m: int, k: int, ids_ptr: int, kstride: int,
+                               ef: int = 0, ef_ptr: int = 0, k_ptr: int = 0, stats_ptr: int = 0,
+                               stream: int = 0) -> None:
+        check(lib().lqg_fs_search_batch_device(self.handle, q_ptr, m, k_ptr or None, k,
+                                               ef_ptr or None, ef, ids_ptr, kstride,
+                                               stats_ptr or None, stream or None))
+
+    def fastscan_status(self, stream: int = 0) -> None:
+        check(lib().lqg_fs_stream_status(self.handle, stream or None))
+
     # Device-pointer entry points (pointers as ints; stream as int handle).
     def search_device(self, q_ptr: int, m: int, k: int, ids_ptr: int, kstride: int, ef: int = 0,
                       ef_ptr: int = 0, k_ptr: int = 0, pool_ids_ptr: int = 0,
