@@ -671,6 +671,8 @@ def gpu_arm(args, w, name, rank, world, device):
         # best-10-of-pool recall, the algorithmic roofline fraction of the
         # search kernel and its ids against the reference on a sample
         extra["grid"] = grid_points(ix, w, name, path, queries, q_dev, gt, flush, stream, peak)
+        # the upstream FastScan/RaBitQ search on the same graph, beside the SQ8 path
+        extra["fastscan"] = fastscan_leg(ix, w, queries, q_dev, gt, flush, stream, peak)
         # the same search on a 4x larger batch (these queries and three more
         # query seeds of the workload), L2 flushed: the kernel's throughput
         # with less of the batch's ramp and tail per query
@@ -820,6 +822,70 @@ def grid_points(ix, w, name, path, queries, q_dev, gt, flush, stream, peak):
                 "ids_mismatch_vs_reference": int((ref_ids != got).any(1).sum()),
                 "reference_sample": f"first {sample} queries ({kind})"}
             log(f"[grid] k={k} ef={ef}: {out[f'k{k}_ef{ef}']}")
+    return out
+
+
+def fastscan_leg(ix, w, queries, q_dev, gt, flush, stream, peak):
+    """The upstream FastScan/RaBitQ search (search_qg with an exact re-rank of
+    every popped node) on the headline index: its section encoded on the GPU
+    (lqg_fs_build), then for each ef: device-resident QPS (L2 flushed),
+    recall@10 of its k = 10 output, the roofline fraction of its algorithmic
+    bytes (one row per expanded node, a vector and ids row per update_results
+    evaluation, the query), ids against the reference's own search_qg on a
+    sample, and that reference's CPU throughput on all host cores."""
+    import torch
+
+    from oracle.oracle import RefFastScan, ref_available
+
+    nq, dim, deg = len(queries), w["dim"], w["deg"]
+    sh = stream.cuda_stream
+    dev = q_dev.device
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    ix.fastscan_build(seed=0)
+    enc_s = time.perf_counter() - t
+    diag, packed, fac = ix.fastscan_arrays()
+    P = len(diag)
+    row_bytes = 4 * ((dim + 3) & ~3) + deg * P // 8 + 16 * deg
+    ref = None
+    if ref_available():
+        _, vecs, nbrs, _, _ = ix.get_arrays()
+        ref = RefFastScan().open(w["n"], dim, deg, ix.entry_point(), vecs, nbrs, packed, fac, diag)
+        del vecs
+    del packed, fac
+    k = 10
+    out = {"encode_s": enc_s, "row_bytes": row_bytes, "padded_dim": P, "points": {}}
+    ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+    st = torch.zeros((nq, 4), dtype=torch.int32, device=dev)
+    nthreads = os.cpu_count() or 1
+    for ef in (16, 32, 64, 128):
+        def run():
+            ix.search_fastscan_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=ef,
+                                      stats_ptr=st.data_ptr(), stream=sh)
+
+        for _ in range(2):
+            run()
+        ix.fastscan_status(sh)
+        ms = _timed(run, 5, flush, stream)
+        ix.fastscan_status(sh)
+        got = ids.cpu().numpy().view(np.uint32)
+        stx = st.cpu().numpy().astype(np.int64)
+        bytes_launch = float((stx[:, 1] * row_bytes + stx[:, 2] * (4 * dim + 4 * deg) + 4 * dim).sum())
+        pt = {"qps": nq / (ms / 1e3), "ms": ms, "recall_at_10": recall_at(got, gt, 10),
+              "roofline_frac": bytes_launch / (ms / 1e3) / 1e9 / peak,
+              "algorithmic_bytes_per_launch": bytes_launch,
+              "expanded_mean": float(stx[:, 1].mean()), "pops_mean": float(stx[:, 0].mean())}
+        if ref is not None:
+            sample = min(1000, nq)
+            r_ids = ref.search(queries[:sample], k, ef, nthreads)
+            pt["ids_mismatch_vs_reference"] = int((r_ids != got[:sample]).any(1).sum())
+            qps, m, dt, _ = time_cpu(lambda qq: ref.search(qq, k, ef, nthreads), queries, 3.0)
+            pt["cpu_reference_qps"] = qps
+            pt["cpu_reference_sample"] = f"first {m} queries, {nthreads} threads, {dt:.1f}s"
+        out["points"][str(ef)] = pt
+        log(f"[fastscan] ef={ef}: {pt}")
+    if ref is not None:
+        ref.close()
     return out
 
 

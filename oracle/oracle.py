@@ -461,18 +461,44 @@ class RefFastScan:
                              _ptr(packed), _ptr(factors), _ptr(out))
         return out
 
+    def open(self, n, dim, deg, entry, vectors, nbrs, packed, factors, diag):
+        """The reference's QuantizedGraph with upstream's row layout, filled from
+        arrays (packed codes in the FastScan block layout)."""
+        return _RefFsIndex(self, n, dim, deg, entry, vectors, nbrs, packed, factors, diag)
+
     def search(self, fs: FsArrays, q, k, ef, nthreads=0):
         o = FsOracle()
-        P = fs.P
         packed = np.stack([o.pack(fs.codes[i]) for i in range(fs.n)])
-        keep = (np.ascontiguousarray(fs.vectors, np.float32), np.ascontiguousarray(fs.nbrs, np.uint32),
-                packed, np.ascontiguousarray(fs.factors, np.float32),
-                np.ascontiguousarray(fs.diag, np.float32))
-        h = self.lib.ref_fs_open(fs.n, fs.dim, fs.deg, fs.entry, *[_ptr(a) for a in keep])
+        h = self.open(fs.n, fs.dim, fs.deg, fs.entry, fs.vectors, fs.nbrs, packed, fs.factors,
+                      fs.diag)
         try:
-            q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
-            out = np.zeros((q.shape[0], k), np.uint32)
-            self.lib.ref_fs_search(h, _ptr(q), q.shape[0], k, ef, _ptr(out), nthreads)
+            return h.search(q, k, ef, nthreads)
         finally:
-            self.lib.ref_fs_close(h)
+            h.close()
+
+
+class _RefFsIndex:
+    def __init__(self, r: RefFastScan, n, dim, deg, entry, vectors, nbrs, packed, factors, diag):
+        self.r, self.dim = r, dim
+        keep = (np.ascontiguousarray(vectors, np.float32), np.ascontiguousarray(nbrs, np.uint32),
+                np.ascontiguousarray(packed, np.uint8), np.ascontiguousarray(factors, np.float32),
+                np.ascontiguousarray(diag, np.float32))
+        self.handle = r.lib.ref_fs_open(n, dim, deg, entry, *[_ptr(a) for a in keep])
+
+    def search(self, q, k, ef, nthreads=0):
+        """The reference's search() with search_qg, per query, on nthreads threads."""
+        q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+        out = np.zeros((q.shape[0], k), np.uint32)
+        self.r.lib.ref_fs_search(self.handle, _ptr(q), q.shape[0], k, ef, _ptr(out), nthreads)
         return out
+
+    def close(self):
+        if self.handle:
+            self.r.lib.ref_fs_close(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
