@@ -63,7 +63,8 @@ LQG_API lqg_status lqg_create(const char* index_type, const char* metric,
 LQG_API void lqg_free(lqg_index* ix);
 
 /* Index.load: symqglib/qg/qg.hpp:217-224. The file must be exactly
- * 4 + 4*N*(D+deg) + N*D + 8*D bytes; every neighbour id must be < N.
+ * 4 + 4*N*(D+deg) + N*D + 8*D bytes, optionally followed by a FastScan
+ * section (see lqg_fs_build); every neighbour id must be < N.
  * Uploads the neighbour lists, codes and SQ8 parameters to the device. */
 LQG_API lqg_status lqg_load(lqg_index* ix, const char* path);
 
@@ -259,19 +260,23 @@ LQG_API lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t);
  * dispatcher launches whatever is pending as one batch as soon as one of
  * `streams` contexts is free, so requests that arrive while other batches
  * are on the GPU are admitted as contexts free up and overlap with them.
- * Each context holds the device state of at most `max_batch` requests
- * (query, k, ef, ids, plus its own work areas); max_batch defaults to what
- * `state_budget` bytes (default 256 MiB) allow. Start runs one full-size
- * batch on every context (max_batch queries at max_k and max_ef, in the
- * index's current tuning mode) so that the contexts' work areas are at their
- * largest before the first request: growing them later would allocate device
- * memory, which waits for the whole device. Set the tuning before starting.
+ * Admission is by each request's own device state (query, k, ef, ids, and
+ * the per-query candidate logs, sized by its ef): requests fall in ef classes
+ * (<= 64, 128, 256, 512); a batch takes the oldest pending request and every
+ * pending request of the same or a smaller class, in arrival order, up to
+ * the count of that class whose state fits the context's share
+ * (state_budget / streams, default budget 256 MiB); `max_batch`, if set,
+ * caps every class. Start runs one full-size batch of every class on every
+ * context (in the index's current tuning mode) so that the contexts' work
+ * areas are at their largest before the first request: growing them later
+ * would allocate device memory, which waits for the whole device. Set the
+ * tuning before starting. A batch's state is released when its batch ends.
  * Results are exactly those of a search of the query alone. While a server
  * runs, use the index only through it. */
 typedef struct lqg_server lqg_server;
 typedef struct {
     uint32_t streams;      /* contexts (batches in flight), default 4 */
-    uint32_t max_batch;    /* requests per batch, default from state_budget */
+    uint32_t max_batch;    /* cap on requests per batch (0: from state_budget per class) */
     uint64_t state_budget; /* device bytes for admitted requests, default 256 MiB */
     uint32_t max_k;        /* largest k of a request, default 100 */
     uint32_t max_ef;       /* largest ef of a request, default 512 */
@@ -282,7 +287,7 @@ typedef struct {
     double mean_batch;
     double p50_us, p99_us; /* latency submit -> result */
     double qps;            /* completed / elapsed */
-    uint32_t max_batch, streams;
+    uint32_t max_batch, streams;  /* max_batch: the largest class's count */
 } lqg_server_metrics;
 
 LQG_API lqg_status lqg_server_start(lqg_index* ix, const lqg_server_config* cfg,

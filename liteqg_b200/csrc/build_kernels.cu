@@ -298,15 +298,20 @@ __device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16]) {
 //     candidates in distance order (the spirit of graph_refine,
 //     qg_builder.hpp:293-348) and mark the row count; rest rows receive the
 //     pruned candidates for a later fill.
+// TC selects the candidate-to-candidate distance form at compile time (1:
+// BF16 Gram matrices on the tensor cores, 0: FP32 on the CUDA cores), so
+// each instance holds only its own path's registers.
+template <int TC>
 __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t s_ids[kCandMax];
     __shared__ float s_d[kCandMax];
     __shared__ uint32_t s_cnt;
-    __shared__ uint8_t s_state[kPruneMax];  // 0 open, 2 pruned
     __shared__ uint8_t s_keep[kPruneMax];   // 1 kept
-    float* tile = reinterpret_cast<float*>(smem);                 // [kPruneMax+1][kTileD+1]
-    float* pair = tile + (kPruneMax + 1) * (kTileD + 1);            // [kPruneMax][kPruneMax]
+    // FP32 path: tile [kPruneMax+1][kTileD+1] floats; tensor-core path: the
+    // BF16 operand, 128 rows x kTileD; then pair [kPruneMax][kPruneMax]
+    float* tile = reinterpret_cast<float*>(smem);
+    float* pair = tile + (TC ? 128 * kTileD / 2 : (kPruneMax + 1) * (kTileD + 1));
 
     const uint64_t node = blockIdx.x + a.node0;
     if (node >= a.n) return;
@@ -439,7 +444,7 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     __shared__ float s_norm[128];
     __shared__ int s_exact;
     if (tid == 0) s_exact = 0;
-    if (a.pair_tc) {
+    if constexpr (TC != 0) {
         // BF16 Gram matrices on the tensor cores (see tc:: above)
         __nv_bfloat16* op = reinterpret_cast<__nv_bfloat16*>(tile);  // 128 rows x 128 dims, 32 KB
         if (tid < 32) {
@@ -585,57 +590,66 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
             if (p < npairs) pair[(pab[s] & 0xFFFFu) * kPruneMax + (pab[s] >> 16)] = acc[s];
         }
     }
-    for (uint32_t i = tid; i < kPruneMax; i += kPruneThreads) {
-        s_state[i] = 0;
-        s_keep[i] = 0;
+    // 5a. every pair's occlusion decision at once: kept j would prune later i
+    // when alpha^2 d(j, i) < d(node, i). The BF16 estimate decides unless it
+    // lies within its error bound of the threshold; then the FP32 value, in
+    // the same order as the CUDA-core path, decides. A decision does not
+    // depend on which candidates the greedy pass keeps, so all pairs are
+    // decided in parallel, one bit each, with no barrier per kept neighbour.
+    constexpr uint32_t kOccW = (kPruneMax + 31) / 32;
+    __shared__ uint32_t s_occ[kPruneMax][kOccW];
+    for (uint32_t i = tid; i < (uint32_t)kPruneMax * kOccW; i += kPruneThreads)
+        (&s_occ[0][0])[i] = 0;
+    for (uint32_t i = tid; i < kPruneMax; i += kPruneThreads) s_keep[i] = 0;
+    __syncthreads();
+    for (uint32_t e = tid; e < P * P; e += kPruneThreads) {
+        const uint32_t j = e / P, i = e % P;
+        if (i <= j) continue;
+        float dji = pair[j * kPruneMax + i];
+        if (TC && !s_exact) {
+            const float ni = s_norm[i], nj = s_norm[j];
+            const float err = 0.015625f * sqrtf(fmaxf(dji, 0.f)) * (sqrtf(ni) + sqrtf(nj)) +
+                              2.5e-4f * (ni + nj);
+            if (fabsf(a.alpha2 * dji - s_d[i]) <= a.alpha2 * err) {
+                const float* xj = a.x + (uint64_t)(s_ids[j] >> 1) * dim;
+                const float* xi = a.x + (uint64_t)(s_ids[i] >> 1) * dim;
+                float t = 0.f;
+                for (uint32_t d = 0; d < dim; ++d) {
+                    const float df = xj[d] - xi[d];
+                    t = fmaf(df, df, t);
+                }
+                dji = t;
+                if (a.rechecks) atomicAdd(a.rechecks, 1ull);
+            }
+        }
+        if (a.alpha2 * dji < s_d[i]) atomicOr(&s_occ[j][i >> 5], 1u << (i & 31));
     }
     __syncthreads();
 
-    // 5. greedy prune: kept j prunes later i when d(j, i) < d(node, i).
-    // s_state[i] only ever goes 0 -> 2 (pruned), written for i > j by the
-    // thread that owns i and read at the top of later iterations, after the
-    // barrier; kept marks go to s_keep, which the loop never reads; every
-    // thread counts kept candidates in a register, so all threads take the
-    // same branches.
+    // 5b. the greedy pass over the bit rows, in one warp: candidates in
+    // distance order; an open one is kept (within the caps) and prunes what
+    // its row marks.
     const uint32_t cap = a.out_cap ? min(a.out_cap, a.deg) : a.deg;
     // far_budget slots are held for long links: a candidate farther than 4x
     // the nearest one's squared distance; near ones stop at cap - far_budget
     const uint32_t near_cap = a.far_budget < cap ? cap - a.far_budget : cap;
     const float far_d = 4.0f * s_d[0];
-    uint32_t kept_n = 0, kept_near = 0;
-    for (uint32_t j = 0; j < P; ++j) {
-        if (s_state[j] != 0) continue;
-        if (kept_n >= cap) break;
-        const bool is_far = a.far_budget != 0 && s_d[j] > far_d;
-        if (!is_far && kept_near >= near_cap) continue;
-        ++kept_n;
-        if (!is_far) ++kept_near;
-        if (tid == 0) s_keep[j] = 1;
-        for (uint32_t i = j + 1 + tid; i < P; i += kPruneThreads) {
-            if (s_state[i] != 0) continue;
-            float dji = pair[j * kPruneMax + i];
-            if (a.pair_tc && !s_exact) {
-                // the BF16 estimate decides unless it lies within its error
-                // bound of the threshold; then the FP32 value, in the same
-                // order as the CUDA-core path, decides
-                const float ni = s_norm[i], nj = s_norm[j];
-                const float err = 0.015625f * sqrtf(fmaxf(dji, 0.f)) * (sqrtf(ni) + sqrtf(nj)) +
-                                  2.5e-4f * (ni + nj);
-                if (fabsf(a.alpha2 * dji - s_d[i]) <= a.alpha2 * err) {
-                    const float* xj = a.x + (uint64_t)(s_ids[j] >> 1) * dim;
-                    const float* xi = a.x + (uint64_t)(s_ids[i] >> 1) * dim;
-                    float t = 0.f;
-                    for (uint32_t d = 0; d < dim; ++d) {
-                        const float df = xj[d] - xi[d];
-                        t = fmaf(df, df, t);
-                    }
-                    dji = t;
-                    if (a.rechecks) atomicAdd(a.rechecks, 1ull);
-                }
-            }
-            if (a.alpha2 * dji < s_d[i]) s_state[i] = 2;
+    if (tid < 32) {
+        uint32_t pruned[kOccW];
+#pragma unroll
+        for (uint32_t w = 0; w < kOccW; ++w) pruned[w] = 0;
+        uint32_t kept_n = 0, kept_near = 0;
+        for (uint32_t j = 0; j < P; ++j) {
+            if ((pruned[j >> 5] >> (j & 31)) & 1u) continue;
+            if (kept_n >= cap) break;
+            const bool is_far = a.far_budget != 0 && s_d[j] > far_d;
+            if (!is_far && kept_near >= near_cap) continue;
+            ++kept_n;
+            if (!is_far) ++kept_near;
+            if (tid == 0) s_keep[j] = 1;
+#pragma unroll
+            for (uint32_t w = 0; w < kOccW; ++w) pruned[w] |= s_occ[j][w];
         }
-        __syncthreads();
     }
     __syncthreads();
     if (tid == 0) {
@@ -669,8 +683,9 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     }
 }
 
-size_t prune_smem_bytes() {
-    return sizeof(float) * ((size_t)(kPruneMax + 1) * (kTileD + 1) + (size_t)kPruneMax * kPruneMax);
+size_t prune_smem_bytes(int tc) {
+    const size_t tile = tc ? (size_t)128 * kTileD / 2 : (size_t)(kPruneMax + 1) * (kTileD + 1);
+    return sizeof(float) * (tile + (size_t)kPruneMax * kPruneMax);
 }
 
 // Reverse lists as CSR, deterministic: pair (target, source) for every kept
@@ -699,11 +714,11 @@ __global__ void segment_kernel(const uint32_t* __restrict__ keys, uint64_t total
 }
 
 cudaError_t launch_prune(const PruneArgs& a, uint64_t nodes, cudaStream_t st) {
-    const size_t smem = prune_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(prune_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    const size_t smem = prune_smem_bytes(a.pair_tc);
+    auto k = a.pair_tc ? prune_kernel<1> : prune_kernel<0>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    prune_kernel<<<(unsigned)nodes, kPruneThreads, smem, st>>>(a);
+    k<<<(unsigned)nodes, kPruneThreads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

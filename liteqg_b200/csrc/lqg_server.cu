@@ -2,16 +2,25 @@
 // resident index.
 //
 // Requests arrive one at a time (lqg_server_submit, from any host thread).
-// A dispatcher thread takes whatever is pending as soon as one of S stream
-// contexts is free and launches it as one batch on that context's stream;
+// A dispatcher thread takes pending requests as soon as one of S stream
+// contexts is free and launches them as one batch on that context's stream;
 // requests that arrive while batches are on the GPU are admitted into the next
 // free context, so their work overlaps with the batches in flight. A context
 // owns everything a batch mutates on the device (its Workspace: control
-// words, tie list, heap-kernel areas; and staging for up to max_batch
-// requests), which is what admission is measured against: at most
-// S * max_batch requests hold device state at once, sized from the caller's
-// device-memory budget. A completer thread waits for batches in launch order,
-// hands each request its ids and records its latency (submit -> result).
+// words, tie list, heap-kernel areas, per-query result and pop logs; and
+// staging for the requests), which is what admission is measured against.
+//
+// Admission is by each request's own device state: a request's candidate and
+// visited state is sized by its ef (the per-query logs of the batch kernel
+// hold max(1024, 16 ef) entries), so requests are grouped in ef classes
+// (ef <= 64, 128, 256, 512). A batch takes the oldest pending request and,
+// in arrival order, every pending request of the same or a smaller class, up
+// to the number of requests of that class whose state fits the context's
+// share of the device budget. An ef-50 request therefore reserves an ef-64
+// footprint, not an ef-512 one, and short requests are not held behind long
+// ones of a larger class. A completer thread waits for batches in launch
+// order, hands each request its ids and records its latency
+// (submit -> result).
 //
 // Each request is searched by the same kernels and with its own k and ef, so
 // its result is exactly what a batched or single search of that query alone
@@ -67,9 +76,17 @@ struct Ctx {
 
 }  // namespace
 
+// ef classes of the admission: a request of ef e belongs to the first class
+// whose bound is >= e.
+constexpr uint32_t kEfClass[4] = {64, 128, 256, 512};
+constexpr int kNumClass = 4;
+
 struct lqg_server {
     lqg_index* ix = nullptr;
     lqg_server_config cfg{};
+    uint32_t class_ef[kNumClass] = {};   // ef bound of each class (<= max_ef)
+    uint32_t class_cap[kNumClass] = {};  // requests per batch of each class
+    int nclass = 0;
     std::vector<Ctx> ctx;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -106,6 +123,20 @@ void free_ctx(Ctx& c, int device) {
     c = Ctx{};
 }
 
+int request_class(const lqg_server* s, uint32_t ef) {
+    for (int i = 0; i < s->nclass; ++i)
+        if (ef <= s->class_ef[i]) return i;
+    return s->nclass - 1;
+}
+
+// Device bytes one request of ef bound `efc` holds while its batch runs:
+// staging (query, k, ef, ids) and the batch kernel's per-query result log,
+// pop log and log length.
+size_t request_bytes(const lqg_index* ix, uint32_t max_k, uint32_t efc) {
+    const size_t logs = (size_t)std::max(1024u, 16u * efc);
+    return (size_t)ix->dim * 4 + (size_t)max_k * 4 + 8 + logs * (16 + 8) + 4;
+}
+
 void dispatch_loop(lqg_server* s) {
     cudaSetDevice(s->ix->device);
     const uint32_t dim = s->ix->dim;
@@ -131,9 +162,23 @@ void dispatch_loop(lqg_server* s) {
                     break;
                 }
             c->batch.clear();
-            while (!s->pending.empty() && c->batch.size() < s->cfg.max_batch) {
-                c->batch.push_back(s->pending.front());
+            // the oldest request's class, then every pending request of that
+            // class or a smaller one, in arrival order, up to the class's count
+            const int c0 = request_class(s, s->pending.front()->ef);
+            const uint32_t cap = s->class_cap[c0];
+            std::deque<Request*> rest;
+            while (!s->pending.empty()) {
+                Request* r = s->pending.front();
                 s->pending.pop_front();
+                if (c->batch.size() < cap && request_class(s, r->ef) <= c0)
+                    c->batch.push_back(r);
+                else
+                    rest.push_back(r);
+                if (c->batch.size() == cap) break;
+            }
+            while (!rest.empty()) {  // put the skipped ones back, order kept
+                s->pending.push_front(rest.back());
+                rest.pop_back();
             }
             c->busy = true;
         }
@@ -222,27 +267,30 @@ double percentile(std::vector<double> v, double p) {
     return v[i];
 }
 
-// One full-size batch (max_batch zero queries at max_k and max_ef, in the
-// index's current kernel mode) on context c before serving starts: the work
-// areas a batch grows to fit (result and pop logs, search-heap areas) reach
-// their largest size here. Growing them while serving would free and
-// allocate device memory, which waits for every stream of the device.
+// One full-size batch of every class (its count of zero queries at max_k and
+// the class's ef bound, in the index's current kernel mode) on context c
+// before serving starts: the work areas a batch grows to fit (result and pop
+// logs, work order, search-heap areas) reach their largest size here. Growing
+// them while serving would free and allocate device memory, which waits for
+// every stream of the device.
 lqg_status warm_context(lqg_server* s, Ctx& c) {
-    const uint32_t mb = s->cfg.max_batch;
     const uint32_t dim = s->ix->dim;
-    std::memset(c.h_q, 0, (size_t)mb * dim * sizeof(float));
-    for (uint32_t i = 0; i < mb; ++i) {
-        c.h_k[i] = s->cfg.max_k;
-        c.h_ef[i] = s->cfg.max_ef;
+    for (int ci = 0; ci < s->nclass; ++ci) {
+        const uint32_t mb = s->class_cap[ci];
+        std::memset(c.h_q, 0, (size_t)mb * dim * sizeof(float));
+        for (uint32_t i = 0; i < mb; ++i) {
+            c.h_k[i] = s->cfg.max_k;
+            c.h_ef[i] = s->class_ef[ci];
+        }
+        LQG_CUDA(cudaMemcpyAsync(c.d_q, c.h_q, (size_t)mb * dim * 4, cudaMemcpyHostToDevice, c.st));
+        LQG_CUDA(cudaMemcpyAsync(c.d_k, c.h_k, (size_t)mb * 4, cudaMemcpyHostToDevice, c.st));
+        LQG_CUDA(cudaMemcpyAsync(c.d_ef, c.h_ef, (size_t)mb * 4, cudaMemcpyHostToDevice, c.st));
+        BatchSpec b{c.d_q, (int64_t)mb, c.d_k, 0, c.d_ef, s->class_ef[ci], c.d_ids,
+                    s->cfg.max_k, nullptr, nullptr, 0, nullptr, c.st};
+        const lqg_status st = run_batch(s->ix, c.ws, b, false);
+        if (st != LQG_OK) return st;
+        LQG_CUDA(cudaStreamSynchronize(c.st));
     }
-    LQG_CUDA(cudaMemcpyAsync(c.d_q, c.h_q, (size_t)mb * dim * 4, cudaMemcpyHostToDevice, c.st));
-    LQG_CUDA(cudaMemcpyAsync(c.d_k, c.h_k, (size_t)mb * 4, cudaMemcpyHostToDevice, c.st));
-    LQG_CUDA(cudaMemcpyAsync(c.d_ef, c.h_ef, (size_t)mb * 4, cudaMemcpyHostToDevice, c.st));
-    BatchSpec b{c.d_q, (int64_t)mb, c.d_k, 0, c.d_ef, s->cfg.max_ef, c.d_ids,
-                s->cfg.max_k, nullptr, nullptr, 0, nullptr, c.st};
-    const lqg_status st = run_batch(s->ix, c.ws, b, false);
-    if (st != LQG_OK) return st;
-    LQG_CUDA(cudaStreamSynchronize(c.st));
     return LQG_OK;
 }
 
@@ -260,16 +308,27 @@ lqg_status lqg_server_start(lqg_index* ix, const lqg_server_config* cfg, lqg_ser
     if (c.max_ef == 0) c.max_ef = kMaxEf;
     if (c.max_ef > kMaxEf) return fail(LQG_ERR_ARG, "max_ef must be <= 512");
     if (c.streams > 64) return fail(LQG_ERR_ARG, "streams must be <= 64");
-    const size_t per_req = (size_t)ix->dim * 4 + (size_t)c.max_k * 4 + 8 + 4;
-    if (c.max_batch == 0) {
-        const uint64_t budget = c.state_budget ? c.state_budget : (256ull << 20);
-        c.max_batch = (uint32_t)std::min<uint64_t>(16384, std::max<uint64_t>(1, budget / (per_req * c.streams)));
-    }
     DeviceScope ds(ix->device);
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
     auto* s = new (std::nothrow) lqg_server();
     if (!s) return fail(LQG_ERR_NOMEM, "host allocation failed");
     s->ix = ix;
+    // ef classes up to max_ef; each class's count from the context's share of
+    // the budget and its requests' footprint (max_batch, if set, caps it)
+    const uint64_t budget = c.state_budget ? c.state_budget : (256ull << 20);
+    uint32_t most = 1;
+    for (uint32_t b : kEfClass) {
+        const uint32_t efc = std::min(b, c.max_ef);
+        if (s->nclass > 0 && s->class_ef[s->nclass - 1] >= efc) break;
+        uint64_t cnt = std::max<uint64_t>(1, budget / c.streams / request_bytes(ix, c.max_k, efc));
+        cnt = std::min<uint64_t>(cnt, 16384);
+        if (c.max_batch) cnt = std::min<uint64_t>(cnt, c.max_batch);
+        s->class_ef[s->nclass] = efc;
+        s->class_cap[s->nclass] = (uint32_t)cnt;
+        most = std::max(most, (uint32_t)cnt);
+        ++s->nclass;
+    }
+    c.max_batch = most;  // staging size: the largest class count
     s->cfg = c;
     s->ctx.resize(c.streams);
     for (auto& x : s->ctx) {

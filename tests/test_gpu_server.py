@@ -56,3 +56,29 @@ def test_server_concurrent_submitters(golden):
     want = g["expected"][(100, 10)]
     for i, ids in out.items():
         assert np.array_equal(ids, want[i])
+
+
+def test_server_admission_by_ef_class(golden):
+    """A small device budget: each batch holds only requests of one ef class
+    or smaller ones, as many as fit the class's footprint; results still equal
+    each query searched alone, for every class mixed in one stream of requests."""
+    import liteqg_b200
+    from liteqg_b200.serving import Server
+
+    g = golden["u48"]
+    ix = liteqg_b200.Index("QG", "L2", g["n"], g["dim"], g["deg"])
+    ix.load(g["path"])
+    rng = np.random.default_rng(5)
+    q = np.concatenate([g["queries"]] * 4)
+    m = len(q)
+    ks = rng.choice([1, 10, 50], m).astype(np.uint32)
+    efs = rng.choice([16, 64, 100, 200, 300, 512], m).astype(np.uint32)
+    # about 40 ef-64 requests or 5 ef-512 requests per context
+    with Server(ix, streams=2, state_budget=2 * 40 * (48 * 4 + 100 * 4 + 12 + 1024 * 24)) as srv:
+        ids, lat = srv.replay(q, ks, efs, None)
+        st = srv.stats()
+    assert st["completed"] == m
+    assert st["batches"] >= m // 40
+    for i in range(m):
+        k, ef = int(ks[i]), int(efs[i])
+        assert np.array_equal(ids[i, :k], ix.search(q[i:i + 1], k, ef=ef)[0]), (i, k, ef)
