@@ -71,6 +71,10 @@ WORKLOADS = {
     "build-1m768": dict(n=1_000_000, dim=768, gen="gauss_mixture_unit", clusters=2048, sigma=0.3,
                         deg=64, efb=400, iters=3, random_edges=8, path_take=64, far_budget=8,
                         nq=2000, kind="build", ef=128),
+    # config 4's data at N = 100,000: a build small enough to profile
+    "build-100k768": dict(n=100_000, dim=768, gen="gauss_mixture_unit", clusters=2048, sigma=0.3,
+                          deg=64, efb=400, iters=3, random_edges=8, path_take=64, far_budget=8,
+                          nq=2000, kind="build", ef=128),
     # serving loop, open-loop Poisson arrivals
     "serving-10m96": dict(n=10_000_000, dim=96, gen="gauss_mixture", clusters=4096, sigma=0.25,
                           deg=32, efb=300, iters=3, random_edges=8, path_take=64, far_budget=8,
@@ -534,15 +538,27 @@ def gpu_arm(args, w, name, rank, world, device):
         sh = torch.cuda.current_stream(dev).cuda_stream
         q_dev = torch.from_numpy(queries).to(dev)
         ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
-        ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=ef, stream=sh)
+        if args.fastscan:
+            # the FastScan/RaBitQ search instead (its section encoded first)
+            ix.fastscan_build(seed=0)
+            search = lambda: ix.search_fastscan_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k,
+                                                       ef=ef, stream=sh)
+        else:
+            search = lambda: ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=ef,
+                                              stream=sh)
+        search()
         torch.cuda.synchronize(dev)
         torch.cuda.nvtx.range_push("lqg_profile")
         for _ in range(args.profile):
-            ix.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), k, ef=ef, stream=sh)
+            search()
         torch.cuda.synchronize(dev)
         torch.cuda.nvtx.range_pop()
-        ix.stream_status(sh)
-        log(f"[rank {rank}] profiled {args.profile} steps, mode {c[0]}, ef {ef}")
+        if args.fastscan:
+            ix.fastscan_status(sh)
+        else:
+            ix.stream_status(sh)
+        log(f"[rank {rank}] profiled {args.profile} steps, mode {c[0]}, ef {ef}, "
+            f"fastscan {bool(args.fastscan)}")
         ix.close()
         return
     gt = ground_truth(name, w, base, queries, device, rank)
@@ -916,16 +932,42 @@ def uneven_arm(args, w, name, device):
     base = gen_data(w, "base")
     queries = gen_data(w, "query")
     path, t_build = get_index_file(name, w, base, device)
-    gt = ground_truth(name, w, base, queries, device, 0)
-    del base
-    log(f"[uneven] index + gt ready {time.perf_counter() - t0:.1f}s (build {t_build:.1f}s)")
     n, dim, deg, nq = w["n"], w["dim"], w["deg"], w["nq"]
-    ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
-    ix.load(path)
     rng = np.random.default_rng(2)
     efq = rng.choice(w["ef_choices"], nq).astype(np.uint32)
     kq = rng.choice(w["k_choices"], nq).astype(np.uint32)
     kmax, efmax = int(kq.max()), int(efq.max())
+    if args.profile:
+        # profiling: only the index, the queries and the kernels' work areas
+        # on the device; the launch shape of --mode (default 2, the heap kernel)
+        del base
+        ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
+        ix.load(path)
+        mode = args.mode or 2
+        ix.set_tuning(mode=mode, lanes_per_cand=2, heap_warps=4, heap_scap=512, visited_bits=10)
+        dev = torch.device("cuda", device)
+        sh = torch.cuda.current_stream(dev).cuda_stream
+        q_dev = torch.from_numpy(queries).to(dev)
+        ids = torch.empty((nq, kmax), dtype=torch.int32, device=dev)
+        e_dev = torch.from_numpy(efq.view(np.int32)).to(dev)
+        k_dev = torch.from_numpy(kq.view(np.int32)).to(dev)
+        run = lambda: ix.search_device(q_dev.data_ptr(), nq, 0, ids.data_ptr(), kmax, ef=efmax,
+                                       ef_ptr=e_dev.data_ptr(), k_ptr=k_dev.data_ptr(), stream=sh)
+        run()
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_push("lqg_profile")
+        for _ in range(args.profile):
+            run()
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_pop()
+        ix.stream_status(sh)
+        log(f"[uneven] profiled {args.profile} steps, mode {mode}")
+        return
+    gt = ground_truth(name, w, base, queries, device, 0)
+    del base
+    log(f"[uneven] index + gt ready {time.perf_counter() - t0:.1f}s (build {t_build:.1f}s)")
+    ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
+    ix.load(path)
     # recall: best-10 of each query's pool (untimed)
     _, (pid, _) = ix.search(queries, 10, ef=efq, return_pool=True)
     rec_by_ef = {int(e): recall_at(pid[efq == e], gt[efq == e], 10) for e in w["ef_choices"]}
@@ -1319,6 +1361,8 @@ def main():
     ap.add_argument("--build-only", action="store_true",
                     help="build the workload's index (no cache), print the build report, exit")
     ap.add_argument("--ef", type=int, default=0, help="--profile: the ef to search with")
+    ap.add_argument("--fastscan", action="store_true",
+                    help="--profile: run the FastScan/RaBitQ search instead of the SQ8 search")
     ap.add_argument("--prepare", action="store_true",
                     help="build (or assemble) the workload's cached index file and rank-0 "
                          "ground truth, then exit")

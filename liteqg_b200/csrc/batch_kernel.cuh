@@ -211,8 +211,6 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
         // heap can be rebuilt when the smallest distance is shared.
         bool heap = !ra.lazy;
         uint32_t cur = 0;
-        uint32_t ahead[DEGW];  // look-ahead: the next unpopped node's neighbour ids
-        bool have_ahead = false;
         uint2* plg = ra.plog ? ra.plog + (size_t)qi * ra.rlog_cap : nullptr;
 
         while (!fail) {
@@ -256,16 +254,6 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
                 }
                 __syncwarp();
                 cur = nxt;
-                // Look-ahead: the next unpopped entry is the next pop unless
-                // this expansion accepts something closer. Its neighbour list
-                // is requested now; once it arrives (after this pop's
-                // distances) its neighbours' code rows are asked into L2.
-                if (nxt < alen) {
-                    const uint32_t* nn = a.nbrs + (size_t)ai[nxt] * a.deg;
-#pragma unroll
-                    for (int w = 0; w < DEGW; ++w) ahead[w] = __ldg(nn + w * 32 + lane);
-                    have_ahead = true;
-                }
             }
             ++pops;
 
@@ -308,14 +296,6 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
             for (uint32_t b = 0; b < ncand; b += 32)
                 eval_batch<G, G, LW, 1>(a, cid, cd, b, ncand, qs, pmin, pscale, g, r);
             calcs += ncand;
-            if (have_ahead) {
-#pragma unroll
-                for (int w = 0; w < DEGW; ++w)
-                    if (vis[hash_id(ahead[w], vbits)] != ahead[w])
-                        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.codes + (size_t)ahead[w] *
-                                                                                   a.cstride));
-                have_ahead = false;
-            }
             __syncwarp();
 
             // qg.hpp:329-335: 32 candidates of the list at a time, in order
