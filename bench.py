@@ -59,7 +59,7 @@ WORKLOADS = {
                           k_extra=100),
     "small-100k64": dict(n=100_000, dim=64, gen="uniform", deg=32, efb=200, iters=3,
                          random_edges=4, path_take=64, far_budget=4, nq=1000, k=10,
-                         efs=(20, 40, 60, 100, 200), k_extra=100),
+                         efs=(20, 40, 60, 100, 200), k_extra=100, knn_compare=True),
     # uneven batch, high dimension (per-query ef and k;
     # CUDA-graph replay timed beside the eager launch)
     "uneven-1m960": dict(n=1_000_000, dim=960, gen="gauss_mixture", clusters=256, sigma=0.3,
@@ -579,6 +579,13 @@ def gpu_arm(args, w, name, rank, world, device):
         chosen = w["efs"][-1]
     ix.set_ef(chosen)
     log(f"[rank {rank}] ef={chosen} recall={recall} {time.perf_counter() - t0:.1f}s")
+    knn_recall = None
+    if w.get("knn_compare") and rank == 0:
+        # the same search on the exact deg-NN graph of the same data (same
+        # entry point, codes and parameters): what the builder's candidate
+        # cap and the reference's omitted refine round could at most give
+        knn_recall = knn_graph_recall(ix, w, gen_data(w, "base"), queries, gt, device)
+        log(f"[rank {rank}] exact-kNN-graph recall {knn_recall}")
 
     dev = torch.device("cuda", device)
     stream = torch.cuda.current_stream(dev)
@@ -749,6 +756,7 @@ def gpu_arm(args, w, name, rank, world, device):
         "data": "synthetic",
         "config": {"workload": workload_str(name, w, nq, k, chosen), "ef": chosen, "k": k,
                    "recall_at_10_pool": recall.get(chosen), "recall_by_ef": recall,
+                   **({"recall_by_ef_exact_knn_graph": knn_recall} if knn_recall else {}),
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                    "tuning": tune, "autotune_ms": mode_ms, "tied_query_share": exact_share,
                    "fast_vs_exact_id_mismatch": mismatch, "e2e_ids_equal": e2e_ok,
@@ -780,6 +788,36 @@ def gpu_arm(args, w, name, rank, world, device):
     if rank == 0:
         print(json.dumps(line), flush=True)
     ix.close()
+
+
+def knn_graph_recall(ix, w, base, queries, gt, device):
+    """Best-10-of-pool recall by ef of the same search on the exact deg-NN
+    graph of the base vectors (FP32 on the GPU), entry point, codes and SQ8
+    parameters of `ix`."""
+    import torch
+
+    import liteqg_b200
+
+    dev = torch.device("cuda", device)
+    xb = torch.from_numpy(base).to(dev)
+    nb2 = (xb * xb).sum(1)
+    deg = w["deg"]
+    nbrs = np.empty((len(base), deg), np.uint32)
+    for s0 in range(0, len(base), 4096):
+        q = xb[s0:s0 + 4096]
+        d = nb2[None, :] - 2.0 * (q @ xb.T) + (q * q).sum(1)[:, None]
+        d[torch.arange(len(q), device=dev), torch.arange(s0, s0 + len(q), device=dev)] = float("inf")
+        nbrs[s0:s0 + len(q)] = torch.topk(d, deg, dim=1, largest=False).indices.cpu().numpy()
+    del xb
+    entry, vecs, _, codes, params = ix.get_arrays()
+    kx = liteqg_b200.Index("QG", "L2", w["n"], w["dim"], deg, device=device)
+    kx.set_arrays(entry, vecs, nbrs, codes, params)
+    out = {}
+    for ef in w["efs"]:
+        _, (pid, _) = kx.search(queries, 10, ef=ef, return_pool=True)
+        out[ef] = recall_at(pid, gt, 10)
+    kx.close()
+    return out
 
 
 def grid_points(ix, w, name, path, queries, q_dev, gt, flush, stream, peak):

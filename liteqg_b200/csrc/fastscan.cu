@@ -272,7 +272,7 @@ __device__ __forceinline__ void result_insert(float* rd, uint32_t* ri, uint32_t&
 }
 
 template <int DEGW>
-__global__ void __launch_bounds__(256) fs_search_kernel(FsSearchArgs a) {
+__global__ void __launch_bounds__(256, 4) fs_search_kernel(FsSearchArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -525,7 +525,13 @@ __global__ void __launch_bounds__(256) fs_search_kernel(FsSearchArgs a) {
             uint32_t below[DEGW], pc[DEGW];
             bool acc[DEGW];
 #pragma unroll
-            for (int w = 0; w < DEGW; ++w) below[w] = cand[w] ? count_below(sd, size, y[w]) : 0u;
+            for (int w = 0; w < DEGW; ++w) {
+                // a full buffer whose largest value lies below y_j already
+                // holds ef values under it: j cannot go in, and it lies above
+                // every candidate that can, so it counts for none of them
+                cand[w] = cand[w] && (size < ef || y[w] <= sd[size - 1]);
+                below[w] = cand[w] ? count_below(sd, size, y[w]) : 0u;
+            }
 #pragma unroll
             for (int w = 0; w < DEGW; ++w) {
                 uint32_t c = 0;
