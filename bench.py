@@ -1030,13 +1030,22 @@ def uneven_arm(args, w, name, device):
     # (mode, lanes per candidate, heap warps per block, heap slots, visited bits)
     shapes = ((6, 2, 4, 512, 10), (6, 4, 4, 512, 10), (5, 2, 4, 512, 10), (4, 4, 4, 512, 10),
               (2, 2, 4, 512, 10), (2, 4, 4, 512, 10), (1, 4, 4, 512, 10),
-              (2, 2, 4, 256, 10), (2, 2, 4, 256, 9), (2, 2, 2, 512, 10), (2, 2, 8, 256, 9))
+              (2, 2, 4, 256, 10), (2, 2, 4, 256, 9), (2, 2, 2, 512, 10), (2, 2, 8, 256, 9),
+              # larger visited caches: fewer forgotten nodes evaluated again at
+              # ef up to 512, against fewer resident warps
+              (2, 2, 2, 512, 12), (2, 2, 4, 256, 11), (2, 2, 2, 256, 13), (2, 2, 3, 512, 12))
+    from liteqg_b200._capi import LqgError
+
     for shape in shapes:
         mode, g, hw, scap, vb = shape
         ix.set_tuning(mode=mode, lanes_per_cand=g, heap_warps=hw, heap_scap=scap, visited_bits=vb)
-        for _ in range(2):
-            step()
-        ix.stream_status(sh)
+        try:
+            for _ in range(2):
+                step()
+            ix.stream_status(sh)
+        except LqgError as e:  # a launch shape this index's size cannot take
+            log(f"[uneven] shape {shape} skipped: {e}")
+            continue
         ms = _timed(step, 5, flush, stream)
         log(f"[uneven] mode {mode} G {g} warps {hw} scap {scap} vbits {vb}: {ms:.2f} ms")
         if best is None or ms < best[0]:
