@@ -309,9 +309,10 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     __shared__ uint32_t s_cnt;
     __shared__ uint8_t s_keep[kPruneMax];   // 1 kept
     // FP32 path: tile [kPruneMax+1][kTileD+1] floats; tensor-core path: the
-    // BF16 operand, 128 rows x kTileD; then pair [kPruneMax][kPruneMax]
+    // BF16 hi and lo operands, 128 rows x kTileD each; then pair
+    // [kPruneMax][kPruneMax]
     float* tile = reinterpret_cast<float*>(smem);
-    float* pair = tile + (TC ? 128 * kTileD / 2 : (kPruneMax + 1) * (kTileD + 1));
+    float* pair = tile + (TC ? 128 * kTileD : (kPruneMax + 1) * (kTileD + 1));
 
     const uint64_t node = blockIdx.x + a.node0;
     if (node >= a.n) return;
@@ -445,11 +446,16 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     __shared__ int s_exact;
     if (tid == 0) s_exact = 0;
     if constexpr (TC != 0) {
-        // BF16 Gram matrices on the tensor cores (see tc:: above)
-        __nv_bfloat16* op = reinterpret_cast<__nv_bfloat16*>(tile);  // 128 rows x 128 dims, 32 KB
+        // Gram matrices on the tensor cores (see tc:: above), each centred
+        // value split into BF16 hi + lo (x = hi + lo + r, |r| <= 2^-16 |x|):
+        // G~ = Ghh + Ghl + Ghl^T, two accumulators in tensor memory (columns
+        // 0.. and 128..), so the BF16 error that decides how many decisions
+        // need an FP32 re-check is 2^-16 instead of 2^-8.
+        __nv_bfloat16* op_hi = reinterpret_cast<__nv_bfloat16*>(tile);  // 128 x 128, 32 KB
+        __nv_bfloat16* op_lo = op_hi + 128 * kTileD;                      // 128 x 128, 32 KB
         if (tid < 32) {
             asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                         ::"r"(tc::smem_u32(&s_tmem)), "r"(128u));
+                         ::"r"(tc::smem_u32(&s_tmem)), "r"(256u));
             asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
         }
         if (tid == 0) {
@@ -462,45 +468,57 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         const uint32_t tmem = s_tmem;
         const float* xn = a.x + node * dim;
         const float* xr = a.x + (uint64_t)(s_ids[tid < P ? tid : 0] >> 1) * dim;
-        float nrm = 0.f;
+        float nrm = 0.f;  // |hi|^2 + 2 hi.lo: the Gram diagonal's form
         bool ok = true, rounded = false;
         uint32_t chunk = 0;
         for (uint32_t d0 = 0; d0 < dim; d0 += kTileD, ++chunk) {
-            // row tid of this chunk: bf16(x_candidate - x_node), zero past P and dim
+            // row tid of this chunk: x_candidate - x_node split, zero past P and dim
 #pragma unroll 2
             for (uint32_t kc = 0; kc < kTileD / 8; ++kc) {
-                uint32_t wv[4];
+                uint32_t wh[4], wl[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const uint32_t d = d0 + kc * 8 + 2 * e;
                     float f0 = 0.f, f1 = 0.f;
                     if (tid < P && d < dim) f0 = __fsub_rn(xr[d], xn[d]);
                     if (tid < P && d + 1 < dim) f1 = __fsub_rn(xr[d + 1], xn[d + 1]);
-                    const __nv_bfloat162 b = __floats2bfloat162_rn(f0, f1);
-                    const float r0 = __low2float(b), r1 = __high2float(b);
-                    rounded |= r0 != f0 || r1 != f1;
-                    nrm = __fmaf_rn(r0, r0, nrm);
-                    nrm = __fmaf_rn(r1, r1, nrm);
-                    wv[e] = *reinterpret_cast<const uint32_t*>(&b);
+                    const __nv_bfloat162 h = __floats2bfloat162_rn(f0, f1);
+                    const float h0 = __low2float(h), h1 = __high2float(h);
+                    // f - hi is exact in FP32 (at most 16 significant bits)
+                    const __nv_bfloat162 l =
+                        __floats2bfloat162_rn(__fsub_rn(f0, h0), __fsub_rn(f1, h1));
+                    const float l0 = __low2float(l), l1 = __high2float(l);
+                    rounded |= h0 != f0 || h1 != f1;
+                    nrm = __fmaf_rn(h0, h0, nrm);
+                    nrm = __fmaf_rn(2.f * h0, l0, nrm);
+                    nrm = __fmaf_rn(h1, h1, nrm);
+                    nrm = __fmaf_rn(2.f * h1, l1, nrm);
+                    wh[e] = *reinterpret_cast<const uint32_t*>(&h);
+                    wl[e] = *reinterpret_cast<const uint32_t*>(&l);
                 }
-                *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(op) + kc * 128 +
-                                          (tid >> 3) * 2048 + (tid & 7) * 16) =
-                    make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                const uint32_t off = kc * 128 + (tid >> 3) * 2048 + (tid & 7) * 16;
+                *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(op_hi) + off) =
+                    make_uint4(wh[0], wh[1], wh[2], wh[3]);
+                *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(op_lo) + off) =
+                    make_uint4(wl[0], wl[1], wl[2], wl[3]);
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             if (tid == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t base = tc::smem_u32(op);
+                const uint32_t bh = tc::smem_u32(op_hi), bl = tc::smem_u32(op_lo);
                 constexpr uint32_t idesc = tc::idesc_bf16_f32(128, kPruneMax);
 #pragma unroll
                 for (uint32_t s = 0; s < kTileD / 16; ++s) {
-                    const uint64_t dsc = tc::smem_desc(base + s * 256, 128, 2048);
-                    tc::mma_bf16(tmem, dsc, dsc, idesc, (chunk > 0 || s > 0) ? 1u : 0u);
+                    const uint64_t dh = tc::smem_desc(bh + s * 256, 128, 2048);
+                    const uint64_t dl = tc::smem_desc(bl + s * 256, 128, 2048);
+                    const uint32_t acc = (chunk > 0 || s > 0) ? 1u : 0u;
+                    tc::mma_bf16(tmem, dh, dh, idesc, acc);          // Ghh
+                    tc::mma_bf16(tmem + 128u, dh, dl, idesc, acc);   // Ghl
                 }
                 tc::commit(&s_mbar);
             }
-            // the operand tile is rewritten next chunk: wait for these MMAs
+            // the operand tiles are rewritten next chunk: wait for these MMAs
             if (!tc::mbar_wait(&s_mbar, chunk & 1u)) ok = false;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         }
@@ -510,28 +528,42 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         // distances are exact, so no decision needs a re-check
         const int exact = !__syncthreads_or(rounded || nrm >= 8388608.0f);
         if (tid == 0) s_exact = exact;
-        __syncthreads();
-        // row tid of the Gram matrix -> squared distances to every column
+        // row tid of Ghl into the pair buffer, for its transpose
         const uint32_t w = tid >> 5;
 #pragma unroll 1
         for (uint32_t c0 = 0; c0 < (uint32_t)kPruneMax; c0 += 16) {
             float g[16];
-            tc::ld16(tmem + ((32u * w) << 16) + c0, g);
+            tc::ld16(tmem + ((32u * w) << 16) + 128u + c0, g);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (tid < P)
+#pragma unroll
+                for (int e = 0; e < 16; ++e) pair[tid * kPruneMax + c0 + e] = g[e];
+        }
+        __syncthreads();
+        // squared distances of row tid to the later columns: the upper
+        // triangle is rewritten while only the lower one is read
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < (uint32_t)kPruneMax; c0 += 16) {
+            float gh[16], gl[16];
+            tc::ld16(tmem + ((32u * w) << 16) + c0, gh);
+            tc::ld16(tmem + ((32u * w) << 16) + 128u + c0, gl);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (tid < P) {
 #pragma unroll
                 for (int e = 0; e < 16; ++e) {
                     const uint32_t c = c0 + e;
-                    if (c < P && c > tid)
+                    if (c < P && c > tid) {
+                        const float gt = __fadd_rn(__fadd_rn(gh[e], gl[e]), pair[c * kPruneMax + tid]);
                         pair[tid * kPruneMax + c] =
-                            fmaxf(0.f, __fsub_rn(__fadd_rn(nrm, s_norm[c]), 2.f * g[e]));
+                            fmaxf(0.f, __fsub_rn(__fadd_rn(nrm, s_norm[c]), 2.f * gt));
+                    }
                 }
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         if (tid < 32) {
-            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u));
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
         }
         if (!ok && tid == 0 && a.err) atomicOr(a.err, 1u);
     } else {
@@ -614,9 +646,13 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         if (i <= j) continue;
         const float dji = pair[j * kPruneMax + i];
         if (TC && !s_exact) {
+            // bound on |estimate - FP32 value|: the split's residuals
+            // (2^-15 sqrt(d) (|a| + |b|)), the missing lo.lo term (2^-15 (na + nb)),
+            // FP32 accumulation in tensor memory and in the FP32 path (about
+            // 2 D 2^-24 (na + nb) each), with a factor of 2 to spare
             const float ni = s_norm[i], nj = s_norm[j];
-            const float err = 0.015625f * sqrtf(fmaxf(dji, 0.f)) * (sqrtf(ni) + sqrtf(nj)) +
-                              2.5e-4f * (ni + nj);
+            const float err = 6.103515625e-05f * sqrtf(fmaxf(dji, 0.f)) * (sqrtf(ni) + sqrtf(nj)) +
+                              (2.384185791015625e-07f * (float)dim + 1.220703125e-04f) * (ni + nj);
             if (fabsf(a.alpha2 * dji - s_d[i]) <= a.alpha2 * err) {
                 atomicOr(&s_unc[j][i >> 5], 1u << (i & 31));
                 continue;
@@ -719,7 +755,7 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
 }
 
 size_t prune_smem_bytes(int tc) {
-    const size_t tile = tc ? (size_t)128 * kTileD / 2 : (size_t)(kPruneMax + 1) * (kTileD + 1);
+    const size_t tile = tc ? (size_t)128 * kTileD : (size_t)(kPruneMax + 1) * (kTileD + 1);
     return sizeof(float) * (tile + (size_t)kPruneMax * kPruneMax);
 }
 
