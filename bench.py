@@ -50,7 +50,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "QPS @ recall@10≥0.95: batched vs plain GPU vs CPU; p50/p99 ms; HBM GB/s"
-BUILDER_VERSION = "gpu-builder-4"
+BUILDER_VERSION = "gpu-builder-5"
 
 WORKLOADS = {
     "batched-1m128": dict(n=1_000_000, dim=128, gen="int_mixture", clusters=1024, lo=0.0,

@@ -108,10 +108,10 @@ LQG_API lqg_status lqg_build(lqg_index* ix, const float* data, uint32_t ef_build
  * With reverse edges these become routes from the entry region into every
  * cluster of clustered data.
  *   pair_kernel  candidate-to-candidate distances of the prune: 0 FP32 on the
- *                CUDA cores; 1 BF16 Gram matrices on the tensor cores
- *                (tcgen05, FP32 accumulation in tensor memory) with every
- *                prune decision near its threshold re-checked in FP32, which
- *                gives the same graph as 0.
+ *                CUDA cores; 1 Gram matrices on the tensor cores (tcgen05,
+ *                each value split into BF16 hi + lo, FP32 accumulation in
+ *                tensor memory) with every prune decision near its threshold
+ *                re-checked in FP32, which gives the same graph as 0.
  *   report       optional: prune kernel time and FP32 re-checks of the build. */
 typedef struct {
     double prune_ms;    /* all prune launches (CUDA events) */
@@ -265,7 +265,7 @@ LQG_API lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t);
  * (<= 64, 128, 256, 512); a batch takes the oldest pending request and every
  * pending request of the same or a smaller class, in arrival order, up to
  * the count of that class whose state fits the context's share
- * (state_budget / streams, default budget 256 MiB); `max_batch`, if set,
+ * (state_budget / streams, default budget 4 GiB); `max_batch`, if set,
  * caps every class. Start runs one full-size batch of every class on every
  * context (in the index's current tuning mode) so that the contexts' work
  * areas are at their largest before the first request: growing them later
@@ -277,7 +277,7 @@ typedef struct lqg_server lqg_server;
 typedef struct {
     uint32_t streams;      /* contexts (batches in flight), default 4 */
     uint32_t max_batch;    /* cap on requests per batch (0: from state_budget per class) */
-    uint64_t state_budget; /* device bytes for admitted requests, default 256 MiB */
+    uint64_t state_budget; /* device bytes for admitted requests, default 4 GiB */
     uint32_t max_k;        /* largest k of a request, default 100 */
     uint32_t max_ef;       /* largest ef of a request, default 512 */
 } lqg_server_config;

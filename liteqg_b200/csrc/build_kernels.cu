@@ -30,6 +30,13 @@
 namespace lqg {
 
 // ---- SQ8 encode ---------------------------------------------------------
+//
+// The per-dimension min and max follow std::min / std::max over the rows in
+// order (quantization/sq8.hpp:13-17): a value replaces the current one only
+// when strictly smaller (larger), so among equal values the first row's is
+// kept. That decides the sign of a zero minimum (-0.0 and 0.0 compare equal)
+// and so the file's bytes. Each block scans its rows in order, then the
+// blocks are combined in order.
 
 __global__ void minmax_partial_kernel(const float* __restrict__ x, uint64_t n, uint32_t dim,
                                       uint64_t rows_per_block, float* __restrict__ pmin,
@@ -38,10 +45,11 @@ __global__ void minmax_partial_kernel(const float* __restrict__ x, uint64_t n, u
     const uint64_t r1 = min(n, r0 + rows_per_block);
     for (uint32_t d = threadIdx.x; d < dim; d += blockDim.x) {
         float mn = CUDART_INF_F, mx = -CUDART_INF_F;
-        for (uint64_t i = r0; i < r1; ++i) {
+        if (r0 < r1) mn = mx = x[r0 * dim + d];
+        for (uint64_t i = r0 + 1; i < r1; ++i) {
             const float v = x[i * dim + d];
-            mn = fminf(mn, v);
-            mx = fmaxf(mx, v);
+            if (v < mn) mn = v;
+            if (v > mx) mx = v;
         }
         pmin[(size_t)blockIdx.x * dim + d] = mn;
         pmax[(size_t)blockIdx.x * dim + d] = mx;
@@ -51,10 +59,11 @@ __global__ void minmax_partial_kernel(const float* __restrict__ x, uint64_t n, u
 __global__ void minmax_final_kernel(const float* __restrict__ pmin, const float* __restrict__ pmax,
                                     uint32_t nblocks, uint32_t dim, float* __restrict__ params) {
     for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < dim; d += gridDim.x * blockDim.x) {
-        float mn = CUDART_INF_F, mx = -CUDART_INF_F;
-        for (uint32_t b = 0; b < nblocks; ++b) {
-            mn = fminf(mn, pmin[(size_t)b * dim + d]);
-            mx = fmaxf(mx, pmax[(size_t)b * dim + d]);
+        float mn = pmin[d], mx = pmax[d];
+        for (uint32_t b = 1; b < nblocks; ++b) {
+            const float lo = pmin[(size_t)b * dim + d], hi = pmax[(size_t)b * dim + d];
+            if (lo < mn) mn = lo;
+            if (hi > mx) mx = hi;
         }
         params[2 * d] = mn;
         params[2 * d + 1] = __fmul_rn(__fsub_rn(mx, mn), 1.0f / 255.0f);
@@ -622,57 +631,57 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
             if (p < npairs) pair[(pab[s] & 0xFFFFu) * kPruneMax + (pab[s] >> 16)] = acc[s];
         }
     }
-    // 5a. every pair's occlusion decision at once where it is certain: kept j
-    // would prune later i when alpha^2 d(j, i) < d(node, i). On the tensor-core
-    // path the BF16 estimate decides unless it lies within its error bound of
-    // the threshold; such pairs are marked uncertain, and only those the
-    // greedy pass reaches (j kept, i still open) are re-checked, with the FP32
-    // value in the same order as the CUDA-core path. A decision does not
-    // depend on which candidates the pass keeps, so the certain ones are made
-    // in parallel, one bit each.
+    // 5a. every pair's occlusion decision at once: kept j would prune later i
+    // when alpha^2 d(j, i) < d(node, i). On the tensor-core path the split-
+    // BF16 estimate decides unless it lies within its error bound of the
+    // threshold; then the FP32 value, in the same order as the CUDA-core path,
+    // decides. A decision does not depend on which candidates the greedy pass
+    // keeps, so all pairs are decided in parallel, one bit each, with no
+    // barrier per kept neighbour (the narrow bound leaves few re-checks, and
+    // they run spread over the whole block).
     constexpr uint32_t kOccW = (kPruneMax + 31) / 32;
-    __shared__ uint32_t s_occ[kPruneMax][kOccW];  // certain: j prunes i
-    __shared__ uint32_t s_unc[kPruneMax][kOccW];  // uncertain: re-check if reached
-    __shared__ uint32_t s_res[kPruneMax][kOccW];  // re-check outcomes, row j
-    for (uint32_t i = tid; i < (uint32_t)kPruneMax * kOccW; i += kPruneThreads) {
+    __shared__ uint32_t s_occ[kPruneMax][kOccW];
+    for (uint32_t i = tid; i < (uint32_t)kPruneMax * kOccW; i += kPruneThreads)
         (&s_occ[0][0])[i] = 0;
-        (&s_unc[0][0])[i] = 0;
-        (&s_res[0][0])[i] = 0;
-    }
     for (uint32_t i = tid; i < kPruneMax; i += kPruneThreads) s_keep[i] = 0;
     __syncthreads();
     for (uint32_t e = tid; e < P * P; e += kPruneThreads) {
         const uint32_t j = e / P, i = e % P;
         if (i <= j) continue;
-        const float dji = pair[j * kPruneMax + i];
+        float dji = pair[j * kPruneMax + i];
         if (TC && !s_exact) {
             // bound on |estimate - FP32 value|: the split's residuals
-            // (2^-15 sqrt(d) (|a| + |b|)), the missing lo.lo term (2^-15 (na + nb)),
-            // FP32 accumulation in tensor memory and in the FP32 path (about
-            // 2 D 2^-24 (na + nb) each), with a factor of 2 to spare
+            // (2^-15 sqrt(d) (|a| + |b|)), the missing lo.lo term
+            // (2^-15 (na + nb)), FP32 accumulation in tensor memory and in the
+            // FP32 path (about 2 D 2^-24 (na + nb) each), with a factor of 2 to spare
             const float ni = s_norm[i], nj = s_norm[j];
             const float err = 6.103515625e-05f * sqrtf(fmaxf(dji, 0.f)) * (sqrtf(ni) + sqrtf(nj)) +
                               (2.384185791015625e-07f * (float)dim + 1.220703125e-04f) * (ni + nj);
             if (fabsf(a.alpha2 * dji - s_d[i]) <= a.alpha2 * err) {
-                atomicOr(&s_unc[j][i >> 5], 1u << (i & 31));
-                continue;
+                const float* xj = a.x + (uint64_t)(s_ids[j] >> 1) * dim;
+                const float* xi = a.x + (uint64_t)(s_ids[i] >> 1) * dim;
+                float t = 0.f;
+                for (uint32_t d = 0; d < dim; ++d) {
+                    const float df = xj[d] - xi[d];
+                    t = fmaf(df, df, t);
+                }
+                dji = t;
+                if (a.rechecks) atomicAdd(a.rechecks, 1ull);
             }
         }
         if (a.alpha2 * dji < s_d[i]) atomicOr(&s_occ[j][i >> 5], 1u << (i & 31));
     }
     __syncthreads();
 
-    // 5b. the greedy pass over the bit rows: candidates in distance order; an
-    // open one is kept (within the caps) and prunes what its row marks. Every
-    // thread runs the same pass on the same bits (warp-uniform, no barrier);
-    // a kept candidate with uncertain open pairs has them re-checked by the
-    // whole block, one pair per thread, then one barrier.
+    // 5b. the greedy pass over the bit rows, in one warp: candidates in
+    // distance order; an open one is kept (within the caps) and prunes what
+    // its row marks.
     const uint32_t cap = a.out_cap ? min(a.out_cap, a.deg) : a.deg;
     // far_budget slots are held for long links: a candidate farther than 4x
     // the nearest one's squared distance; near ones stop at cap - far_budget
     const uint32_t near_cap = a.far_budget < cap ? cap - a.far_budget : cap;
     const float far_d = 4.0f * s_d[0];
-    {
+    if (tid < 32) {
         uint32_t pruned[kOccW];
 #pragma unroll
         for (uint32_t w = 0; w < kOccW; ++w) pruned[w] = 0;
@@ -687,39 +696,6 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
             if (tid == 0) s_keep[j] = 1;
 #pragma unroll
             for (uint32_t w = 0; w < kOccW; ++w) pruned[w] |= s_occ[j][w];
-            if constexpr (TC == 0) continue;  // every decision is certain
-            uint32_t u[kOccW], nu = 0;
-#pragma unroll
-            for (uint32_t w = 0; w < kOccW; ++w) {
-                u[w] = s_unc[j][w] & ~pruned[w];
-                nu += __popc(u[w]);
-            }
-            if (nu == 0) continue;  // the same in every thread
-            // the t-th uncertain open pair goes to thread t (nu <= kPruneMax)
-            uint32_t t = 0;
-#pragma unroll
-            for (uint32_t w = 0; w < kOccW; ++w) {
-                uint32_t bm = u[w];
-                while (bm) {
-                    const uint32_t i = w * 32 + __ffs(bm) - 1;
-                    bm &= bm - 1;
-                    if (t == (uint32_t)tid) {
-                        const float* xj = a.x + (uint64_t)(s_ids[j] >> 1) * dim;
-                        const float* xi = a.x + (uint64_t)(s_ids[i] >> 1) * dim;
-                        float dv = 0.f;
-                        for (uint32_t d = 0; d < dim; ++d) {
-                            const float df = xj[d] - xi[d];
-                            dv = fmaf(df, df, dv);
-                        }
-                        if (a.alpha2 * dv < s_d[i]) atomicOr(&s_res[j][i >> 5], 1u << (i & 31));
-                        if (a.rechecks) atomicAdd(a.rechecks, 1ull);
-                    }
-                    ++t;
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (uint32_t w = 0; w < kOccW; ++w) pruned[w] |= s_res[j][w];
         }
     }
     __syncthreads();

@@ -315,7 +315,7 @@ lqg_status lqg_server_start(lqg_index* ix, const lqg_server_config* cfg, lqg_ser
     s->ix = ix;
     // ef classes up to max_ef; each class's count from the context's share of
     // the budget and its requests' footprint (max_batch, if set, caps it)
-    const uint64_t budget = c.state_budget ? c.state_budget : (256ull << 20);
+    const uint64_t budget = c.state_budget ? c.state_budget : (4ull << 30);
     uint32_t most = 1;
     for (uint32_t b : kEfClass) {
         const uint32_t efc = std::min(b, c.max_ef);

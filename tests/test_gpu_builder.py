@@ -29,7 +29,7 @@ def test_build_graph_valid_and_searchable(tmp_path, n, dim, deg):
     assert not (nb == np.arange(n, dtype=np.uint32)[:, None]).any()
     # SQ8 encoding equals the reference encoder (pinned by the oracle tests)
     c2, p2 = sq8_quantize(x, 2)
-    assert np.array_equal(codes, c2) and np.array_equal(params, p2)
+    assert np.array_equal(codes, c2) and np.array_equal(params.view(np.uint32), p2.view(np.uint32))
     # entry point: nearest point to the centroid
     cen = (x.astype(np.float64).sum(0) / n).astype(np.float32)
     d = ((x - cen) ** 2).sum(1)
@@ -130,3 +130,25 @@ def test_tensor_core_prune_builds_the_fp32_graph(kind):
         graphs.append(ix.get_arrays()[2])
     assert np.array_equal(graphs[0], graphs[1]), int((graphs[0] != graphs[1]).any(1).sum())
     assert reps[0]["rechecks"] == 0 and reps[1]["prune_ms"] > 0
+
+
+def test_sq8_params_keep_the_first_of_equal_values():
+    """Rounded integer data holds both -0.0 and 0.0: the minimum's sign is the
+    first row's among the equal values, as std::min over the rows in order
+    gives it (sq8.hpp:13-17), so the saved file matches the reference's bytes."""
+    import liteqg_b200
+
+    rng = np.random.default_rng(8)
+    n, dim = 6000, 48
+    x = np.clip(np.rint(rng.normal(0.0, 3.0, (n, dim))), 0, 255).astype(np.float32)
+    x[0, : dim // 2] = -0.0  # the first row decides for half of the columns
+    x[0, dim // 2:] = 0.0
+    x[1, dim // 2:] = -0.0
+    assert (np.signbit(x) & (x == 0)).any(0).all()
+    ix = liteqg_b200.Index("QG", "L2", n, dim, 32)
+    ix.build_index(x, 64, num_iter=2)
+    _, _, _, codes, params = ix.get_arrays()
+    c2, p2 = sq8_quantize(x, 2)
+    assert np.array_equal(codes, c2)
+    assert np.array_equal(params.view(np.uint32), p2.view(np.uint32))
+    assert np.signbit(params[: dim // 2, 0]).all() and not np.signbit(params[dim // 2:, 0]).any()
