@@ -385,6 +385,15 @@ LQG_API lqg_status lqg_fs_search_batch(lqg_index* ix, const float* queries, int6
 LQG_API lqg_status lqg_fs_search(lqg_index* ix, const float* query, uint32_t k,
                                  uint32_t* results);
 
+/* Self-test of the kernels' failure path (no reference counterpart): every
+ * wait in this library's kernels (mbarrier completions of bulk copies and
+ * tensor-core work, waits between warps) is bounded, and on running out the
+ * kernel records an error the host reads and returns; it never traps or
+ * hangs. This launches one warp that waits `tries` times (1..2^20) on an
+ * mbarrier nothing arrives on; *timed_out receives 1 when the wait ran out
+ * (the expected outcome) and the context stays usable. */
+LQG_API lqg_status lqg_selftest_bounded_wait(int device, uint32_t tries, uint32_t* timed_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,7 @@ SIGNATURES = {
     "lqg_fs_search_batch": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_uint32, _vp, C.c_uint32,
                                       _vp, C.c_uint32, _vp, _vp]),
     "lqg_fs_search": (C.c_int, [_vp, _vp, C.c_uint32, _vp]),
+    "lqg_selftest_bounded_wait": (C.c_int, [C.c_int, C.c_uint32, _u32p]),
 }
 
 

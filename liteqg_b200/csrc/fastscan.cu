@@ -156,6 +156,28 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     return false;
 }
 
+// The kernel-side failure path of every bounded wait in this library, made
+// to run out on purpose: an mbarrier that nothing arrives on is waited for
+// `tries` times; the kernel reports the timeout in *out and returns, leaving
+// the context usable.
+__global__ void wait_selftest_kernel(uint32_t tries, uint32_t* out) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) mbar_init(&bar);
+    __syncwarp();
+    bool done = false;
+    for (uint32_t i = 0; i < tries && !done; ++i) {
+        uint32_t d;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            "selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(d)
+            : "r"(smem_addr(&bar)), "r"(0u)
+            : "memory");
+        done = d != 0;
+    }
+    if (threadIdx.x == 0) *out = done ? 0u : 1u;
+}
+
 __device__ __forceinline__ void l2_prefetch_row(const void* src, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
@@ -1266,6 +1288,19 @@ LQG_API lqg_status lqg_fs_search_batch(lqg_index* ix, const float* queries, int6
     if (stats)
         LQG_CUDA(cudaMemcpyAsync(stats, w.d_stats, (size_t)m * 16, cudaMemcpyDeviceToHost, st));
     return fs_status(w, st);
+}
+
+LQG_API lqg_status lqg_selftest_bounded_wait(int device, uint32_t tries, uint32_t* timed_out) {
+    if (!timed_out || tries == 0 || tries > (1u << 20)) return fail(LQG_ERR_ARG, "tries must be in [1, 2^20]");
+    DeviceScope ds(device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    uint32_t* d = nullptr;
+    LQG_CUDA(cudaMalloc(&d, sizeof(uint32_t)));
+    lqg::wait_selftest_kernel<<<1, 32>>>(tries, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(timed_out, d, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? LQG_OK : cuda_fail(e, "bounded-wait self-test");
 }
 
 LQG_API lqg_status lqg_fs_search(lqg_index* ix, const float* query, uint32_t k, uint32_t* results) {
