@@ -931,7 +931,8 @@ def fastscan_leg(ix, w, queries, q_dev, gt, flush, stream, peak):
         pt = {"qps": nq / (ms / 1e3), "ms": ms, "recall_at_10": recall_at(got, gt, 10),
               "roofline_frac": bytes_launch / (ms / 1e3) / 1e9 / peak,
               "algorithmic_bytes_per_launch": bytes_launch,
-              "expanded_mean": float(stx[:, 1].mean()), "pops_mean": float(stx[:, 0].mean())}
+              "expanded_mean": float(stx[:, 1].mean()), "pops_mean": float(stx[:, 0].mean()),
+              "pops_p99": float(np.percentile(stx[:, 0], 99)), "pops_max": int(stx[:, 0].max())}
         if ref is not None:
             sample = min(1000, nq)
             r_ids = ref.search(queries[:sample], k, ef, nthreads)

@@ -32,11 +32,13 @@ namespace lqg {
 // ---- SQ8 encode ---------------------------------------------------------
 //
 // The per-dimension min and max follow std::min / std::max over the rows in
-// order (quantization/sq8.hpp:13-17): a value replaces the current one only
-// when strictly smaller (larger), so among equal values the first row's is
-// kept. That decides the sign of a zero minimum (-0.0 and 0.0 compare equal)
-// and so the file's bytes. Each block scans its rows in order, then the
-// blocks are combined in order.
+// order (quantization/sq8.hpp:13-17) as the reference's -Ofast build compiles
+// them (minss/maxss, new value second): a value replaces the running one
+// unless that one is strictly smaller (larger), so among equal values the
+// last row's is kept. That decides the sign of a zero minimum (-0.0 and 0.0
+// compare equal) and so the file's bytes. Each block folds its rows in order,
+// then the blocks' results are folded in order; the fold keeps the last of
+// the equal values, so it does not depend on where the blocks split.
 
 __global__ void minmax_partial_kernel(const float* __restrict__ x, uint64_t n, uint32_t dim,
                                       uint64_t rows_per_block, float* __restrict__ pmin,
@@ -48,8 +50,8 @@ __global__ void minmax_partial_kernel(const float* __restrict__ x, uint64_t n, u
         if (r0 < r1) mn = mx = x[r0 * dim + d];
         for (uint64_t i = r0 + 1; i < r1; ++i) {
             const float v = x[i * dim + d];
-            if (v < mn) mn = v;
-            if (v > mx) mx = v;
+            mn = mn < v ? mn : v;
+            mx = mx > v ? mx : v;
         }
         pmin[(size_t)blockIdx.x * dim + d] = mn;
         pmax[(size_t)blockIdx.x * dim + d] = mx;
@@ -62,8 +64,8 @@ __global__ void minmax_final_kernel(const float* __restrict__ pmin, const float*
         float mn = pmin[d], mx = pmax[d];
         for (uint32_t b = 1; b < nblocks; ++b) {
             const float lo = pmin[(size_t)b * dim + d], hi = pmax[(size_t)b * dim + d];
-            if (lo < mn) mn = lo;
-            if (hi > mx) mx = hi;
+            mn = mn < lo ? mn : lo;
+            mx = mx > hi ? mx : hi;
         }
         params[2 * d] = mn;
         params[2 * d + 1] = __fmul_rn(__fsub_rn(mx, mn), 1.0f / 255.0f);
@@ -640,11 +642,26 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
     // barrier per kept neighbour (the narrow bound leaves few re-checks, and
     // they run spread over the whole block).
     constexpr uint32_t kOccW = (kPruneMax + 31) / 32;
+    constexpr uint32_t kRecheckCap = 1024;  // uncertain pairs listed per node
     __shared__ uint32_t s_occ[kPruneMax][kOccW];
+    __shared__ uint16_t s_rl[kRecheckCap];   // (j << 7 | i) of uncertain pairs
+    __shared__ uint32_t s_nrl;
     for (uint32_t i = tid; i < (uint32_t)kPruneMax * kOccW; i += kPruneThreads)
         (&s_occ[0][0])[i] = 0;
     for (uint32_t i = tid; i < kPruneMax; i += kPruneThreads) s_keep[i] = 0;
+    if (tid == 0) s_nrl = 0;
     __syncthreads();
+    // the FP32 value of pair (j, i), in the CUDA-core path's order
+    auto fp32_pair = [&](uint32_t j, uint32_t i) {
+        const float* xj = a.x + (uint64_t)(s_ids[j] >> 1) * dim;
+        const float* xi = a.x + (uint64_t)(s_ids[i] >> 1) * dim;
+        float t = 0.f;
+        for (uint32_t d = 0; d < dim; ++d) {
+            const float df = xj[d] - xi[d];
+            t = fmaf(df, df, t);
+        }
+        return t;
+    };
     for (uint32_t e = tid; e < P * P; e += kPruneThreads) {
         const uint32_t j = e / P, i = e % P;
         if (i <= j) continue;
@@ -658,20 +675,30 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
             const float err = 6.103515625e-05f * sqrtf(fmaxf(dji, 0.f)) * (sqrtf(ni) + sqrtf(nj)) +
                               (2.384185791015625e-07f * (float)dim + 1.220703125e-04f) * (ni + nj);
             if (fabsf(a.alpha2 * dji - s_d[i]) <= a.alpha2 * err) {
-                const float* xj = a.x + (uint64_t)(s_ids[j] >> 1) * dim;
-                const float* xi = a.x + (uint64_t)(s_ids[i] >> 1) * dim;
-                float t = 0.f;
-                for (uint32_t d = 0; d < dim; ++d) {
-                    const float df = xj[d] - xi[d];
-                    t = fmaf(df, df, t);
+                // listed, and re-checked below by all threads at once (a
+                // re-check in this loop would keep its warp's other lanes
+                // idle for the whole row); past the list's end, here
+                const uint32_t slot = atomicAdd(&s_nrl, 1u);
+                if (slot < kRecheckCap) {
+                    s_rl[slot] = (uint16_t)((j << 7) | i);
+                    continue;
                 }
-                dji = t;
+                dji = fp32_pair(j, i);
                 if (a.rechecks) atomicAdd(a.rechecks, 1ull);
             }
         }
         if (a.alpha2 * dji < s_d[i]) atomicOr(&s_occ[j][i >> 5], 1u << (i & 31));
     }
     __syncthreads();
+    if (TC) {
+        const uint32_t nrl = min(s_nrl, kRecheckCap);
+        for (uint32_t t = tid; t < nrl; t += kPruneThreads) {
+            const uint32_t j = s_rl[t] >> 7, i = s_rl[t] & 127u;
+            if (a.alpha2 * fp32_pair(j, i) < s_d[i]) atomicOr(&s_occ[j][i >> 5], 1u << (i & 31));
+        }
+        if (a.rechecks && tid == 0 && nrl) atomicAdd(a.rechecks, (unsigned long long)nrl);
+        __syncthreads();
+    }
 
     // 5b. the greedy pass over the bit rows, in one warp: candidates in
     // distance order; an open one is kept (within the caps) and prunes what
@@ -699,33 +726,70 @@ __global__ void __launch_bounds__(kPruneThreads) prune_kernel(PruneArgs a) {
         }
     }
     __syncthreads();
-    if (tid == 0) {
-        uint32_t* out = a.out + node * a.deg;
+    // 5c. the output lists, compacted by warp 0 with ballots: kept ones in
+    // distance order, then (fill) the others, then (rest_fill) the caller's
+    // earlier list without duplicates, all cut at cap
+    if (tid < 32) {
+        constexpr uint32_t kOutMax = 128;  // degree_bound's largest value
+        __shared__ uint32_t s_out[kOutMax];
+        const uint32_t lt = (1u << tid) - 1u;
         uint32_t w = 0;
-        for (uint32_t j = 0; j < P && w < cap; ++j)
-            if (s_keep[j]) out[w++] = s_ids[j] >> 1;
+        for (uint32_t j0 = 0; j0 < P && w < cap; j0 += 32) {
+            const uint32_t j = j0 + tid;
+            const bool take = j < P && s_keep[j];
+            const uint32_t m = __ballot_sync(~0u, take);
+            const uint32_t pos = w + __popc(m & lt);
+            if (take && pos < cap) s_out[pos] = s_ids[j] >> 1;
+            w = min(w + __popc(m), cap);
+        }
         const uint32_t kept = w;
         if (a.fill)
-            for (uint32_t j = 0; j < P && w < cap; ++j)
-                if (!s_keep[j]) out[w++] = s_ids[j] >> 1;
+            for (uint32_t j0 = 0; j0 < P && w < cap; j0 += 32) {
+                const uint32_t j = j0 + tid;
+                const bool take = j < P && !s_keep[j];
+                const uint32_t m = __ballot_sync(~0u, take);
+                const uint32_t pos = w + __popc(m & lt);
+                if (take && pos < cap) s_out[pos] = s_ids[j] >> 1;
+                w = min(w + __popc(m), cap);
+            }
+        __syncwarp();
         if (a.rest_fill) {  // caller's earlier pruned list
             const uint32_t* rr = a.rest_fill + node * a.rest_stride;
             const uint32_t rc = min(a.rest_fill_cnt[node], a.rest_stride);
-            for (uint32_t j = 0; j < rc && w < cap; ++j) {
-                const uint32_t v = rr[j];
-                bool dup = v == (uint32_t)node;
-                for (uint32_t t = 0; t < w && !dup; ++t) dup = out[t] == v;
-                if (!dup) out[w++] = v;
+            for (uint32_t j0 = 0; j0 < rc && w < cap; j0 += 32) {
+                const uint32_t j = j0 + tid;
+                const bool in = j < rc;
+                const uint32_t v = in ? rr[j] : 0xFFFFFFFFu;
+                bool dup = !in || v == (uint32_t)node;
+                for (uint32_t t = 0; t < w && !dup; ++t) dup = s_out[t] == v;
+                // a lower lane with the same id: that one is taken or is itself
+                // a duplicate, so this one is a duplicate either way
+                if (__match_any_sync(~0u, v) & lt) dup = true;
+                const uint32_t m = __ballot_sync(~0u, !dup);
+                const uint32_t pos = w + __popc(m & lt);
+                if (!dup && pos < cap) s_out[pos] = v;
+                w = min(w + __popc(m), cap);
+                __syncwarp();
             }
         }
-        a.out_cnt[node] = w;
-        if (a.kept_cnt) a.kept_cnt[node] = kept;
+        uint32_t* out = a.out + node * a.deg;
+        for (uint32_t t = tid; t < w; t += 32) out[t] = s_out[t];
         if (a.rest) {
             uint32_t* rr = a.rest + node * a.rest_stride;
             uint32_t rw = 0;
-            for (uint32_t j = 0; j < P && rw < a.rest_stride; ++j)
-                if (!s_keep[j]) rr[rw++] = s_ids[j] >> 1;
-            a.rest_cnt[node] = rw;
+            for (uint32_t j0 = 0; j0 < P && rw < a.rest_stride; j0 += 32) {
+                const uint32_t j = j0 + tid;
+                const bool take = j < P && !s_keep[j];
+                const uint32_t m = __ballot_sync(~0u, take);
+                const uint32_t pos = rw + __popc(m & lt);
+                if (take && pos < a.rest_stride) rr[pos] = s_ids[j] >> 1;
+                rw = min(rw + __popc(m), a.rest_stride);
+            }
+            if (tid == 0) a.rest_cnt[node] = rw;
+        }
+        if (tid == 0) {
+            a.out_cnt[node] = w;
+            if (a.kept_cnt) a.kept_cnt[node] = kept;
         }
     }
 }

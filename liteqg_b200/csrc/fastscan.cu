@@ -1014,9 +1014,12 @@ lqg_status fs_run(lqg_index* ix, Workspace& w, const float* q, int64_t m, const 
     a.err = w.d_ctl + kCtlErr;
     a.efcap = ef0;
     a.kcap = kstride;
-    // visited table: popped nodes (about ef of them) and, when ef < k, the
-    // neighbours update_results scans; at most half full
-    uint32_t need = 2 * (ef0 + 64);
+    // visited table: popped nodes and, when ef < k, the neighbours
+    // update_results scans; at most half full. Pops run past ef (about 1.4 ef
+    // on average at ef 64, more in the tail), and a query that fills the
+    // table is searched again in round 1 with one warp per block, which costs
+    // the batch a whole query's latency: room for 2 ef + 64 pops
+    uint32_t need = 2 * (2 * ef0 + 64);
     if (kstride > ef0) need = std::max<uint32_t>(need, 2 * (ef0 + 8 + ix->deg * (kstride + 1)));
     uint32_t vb = 8;
     while ((1u << vb) < need && vb < 12) ++vb;

@@ -48,10 +48,15 @@ void lqgo_sq8_quantize(const float* data, uint64_t dim, uint64_t n,
                        uint8_t* codes, float* params, int recip) {
     for (uint64_t d = 0; d < dim; ++d) {
         float mn = data[d], mx = data[d];
+        /* std::min(min, val) / std::max(max, val) (sq8.hpp:13-17) as the
+         * reference's -Ofast build compiles them: minss/maxss with the new
+         * value second, which returns it unless the running value is strictly
+         * smaller (larger). Among equal values (-0.0 and 0.0) the LAST row's
+         * is kept, and that decides the file's bytes for a zero minimum. */
         for (uint64_t i = 1; i < n; ++i) {
             float v = data[i * dim + d];
-            mn = v < mn ? v : mn;
-            mx = mx < v ? v : mx;
+            mn = mn < v ? mn : v;
+            mx = mx > v ? mx : v;
         }
         float scale = (recip & 2) ? (mx - mn) * (1.0f / 255.0f) : (mx - mn) / 255.0f;
         float inv = 1.0f / scale;

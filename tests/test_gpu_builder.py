@@ -132,23 +132,33 @@ def test_tensor_core_prune_builds_the_fp32_graph(kind):
     assert reps[0]["rechecks"] == 0 and reps[1]["prune_ms"] > 0
 
 
-def test_sq8_params_keep_the_first_of_equal_values():
+def test_sq8_params_keep_the_reference_zero():
     """Rounded integer data holds both -0.0 and 0.0: the minimum's sign is the
-    first row's among the equal values, as std::min over the rows in order
-    gives it (sq8.hpp:13-17), so the saved file matches the reference's bytes."""
+    one the reference's compiled std::min keeps (the last of the equal values
+    over the rows in order, sq8.hpp:13-17), so the saved file matches the
+    reference's bytes; the fixture is the reference's own encoder output."""
+    import os
+
     import liteqg_b200
 
+    from tests.golden.make_sq8_golden import signed_zero_data
+
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             "sq8_signed_zero.npz"))
+    assert np.array_equal(signed_zero_data().view(np.uint32), z["x"].view(np.uint32))
     rng = np.random.default_rng(8)
     n, dim = 6000, 48
     x = np.clip(np.rint(rng.normal(0.0, 3.0, (n, dim))), 0, 255).astype(np.float32)
-    x[0, : dim // 2] = -0.0  # the first row decides for half of the columns
-    x[0, dim // 2:] = 0.0
-    x[1, dim // 2:] = -0.0
+    x[-1, : dim // 2] = -0.0  # the last row decides for half of the columns
+    x[-1, dim // 2:] = 0.0
+    x[-2, dim // 2:] = -0.0
     assert (np.signbit(x) & (x == 0)).any(0).all()
-    ix = liteqg_b200.Index("QG", "L2", n, dim, 32)
-    ix.build_index(x, 64, num_iter=2)
-    _, _, _, codes, params = ix.get_arrays()
-    c2, p2 = sq8_quantize(x, 2)
-    assert np.array_equal(codes, c2)
-    assert np.array_equal(params.view(np.uint32), p2.view(np.uint32))
-    assert np.signbit(params[: dim // 2, 0]).all() and not np.signbit(params[dim // 2:, 0]).any()
+    for data in (z["x"], x):
+        ix = liteqg_b200.Index("QG", "L2", len(data), dim, 32)
+        ix.build_index(data, 64, num_iter=2)
+        _, _, _, codes, params = ix.get_arrays()
+        c2, p2 = sq8_quantize(data, 2)
+        assert np.array_equal(codes, c2)
+        assert np.array_equal(params.view(np.uint32), p2.view(np.uint32))
+        ix.close()
+    assert np.array_equal(params.view(np.uint32)[:, 0] >> 31, (np.arange(dim) < dim // 2))

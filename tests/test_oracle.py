@@ -48,6 +48,31 @@ def test_encoder_matches_reference_file(golden):
         assert np.array_equal(params, ix.params), name
 
 
+def test_encoder_signed_zero_matches_reference_golden():
+    """-0.0 and 0.0 in every column: the oracle keeps the same one as the
+    reference's compiled std::min (the last of the equal values), so the
+    params' bytes agree (fixture: tests/golden/make_sq8_golden.py)."""
+    import os
+
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             "sq8_signed_zero.npz"))
+    codes, params = sq8_quantize(z["x"], recip=2)
+    assert np.array_equal(codes, z["codes"])
+    assert np.array_equal(params.view(np.uint32), z["params"].view(np.uint32))
+    assert np.signbit(params[:24, 0]).all() and not np.signbit(params[24:, 0]).any()
+
+
+@pytest.mark.skipif(not ref_available(), reason="compiled reference (oracle/_ref) not present")
+def test_encoder_signed_zero_matches_reference_random():
+    rng = np.random.default_rng(11)
+    h = RefHarness()
+    for trial in range(4):
+        x = np.clip(np.rint(rng.normal(0.0, 2.0, (700, 40))), 0, 9).astype(np.float32)
+        c1, p1 = h.sq8_quantize(x)
+        c2, p2 = sq8_quantize(x, recip=2)
+        assert np.array_equal(c1, c2) and np.array_equal(p1.view(np.uint32), p2.view(np.uint32))
+
+
 def test_index_roundtrip(golden, tmp_path):
     g = golden["mix128d64"]
     ix = read_index(g["path"], g["n"], g["dim"], g["deg"])
