@@ -239,7 +239,13 @@ LQG_API lqg_status lqg_search_exact_noalloc(lqg_index* ix, const float* queries,
  *   replay_all      modes 4-6: 1 sends every query through the checked result
  *                   replay pass (0, the default: only queries whose output
  *                   the heap layout decides); set on every call, not kept
- *                   when 0 is passed */
+ *                   when 0 is passed
+ *   small_batch     modes 5-6: a batch of at most this many queries runs one
+ *                   query per block of 4 warps (each expansion's distances
+ *                   split over the warps: lower latency per query, fewer
+ *                   queries resident); LQG_SMALL_BATCH_AUTO (the default):
+ *                   as many queries as such blocks fit on the GPU at once;
+ *                   LQG_SMALL_BATCH_OFF: never. The same ids either way. */
 typedef struct {
     uint32_t lanes_per_cand;
     uint32_t visited_bits;
@@ -250,8 +256,11 @@ typedef struct {
     uint32_t heap_scap;
     uint32_t replay_warps;
     uint32_t replay_all;
+    uint32_t small_batch;
 } lqg_tuning;
 
+#define LQG_SMALL_BATCH_AUTO 0xFFFFFFFEu
+#define LQG_SMALL_BATCH_OFF 0xFFFFFFFFu
 LQG_API lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t);
 LQG_API lqg_status lqg_get_tuning(const lqg_index* ix, lqg_tuning* t);
 

@@ -80,7 +80,12 @@ class Tuning(C.Structure):
         ("heap_scap", C.c_uint32),
         ("replay_warps", C.c_uint32),
         ("replay_all", C.c_uint32),
+        ("small_batch", C.c_uint32),
     ]
+
+
+SMALL_BATCH_AUTO = 0xFFFFFFFE
+SMALL_BATCH_OFF = 0xFFFFFFFF
 
 
 class BuildReport(C.Structure):

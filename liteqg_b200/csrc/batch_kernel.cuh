@@ -131,12 +131,26 @@ __device__ __forceinline__ uint32_t upper_rank(const float* a, uint32_t n, float
 constexpr int batch_load_words(int degw) { return degw == 1 ? 16 : 8; }
 constexpr uint32_t kBatchWideDim = 256;
 
-template <int G, int DEGW, int LW>
-__global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, ReplayArgs ra) {
+// Named barriers of the query-per-block form (barrier 0 is __syncthreads).
+__device__ __forceinline__ void named_bar(uint32_t id, uint32_t threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+constexpr uint32_t kCtaStop = 0xFFFFFFFFu;
+
+// H = 0: one warp per query, blocks of up to 5 query warps. H > 0: one query
+// per block of 1 + H warps (the latency form for small batches): warp 0 runs
+// the search as above, and each expansion's distances are split over all the
+// block's warps, 32 / (H + 1) candidates each, one round of code loads for
+// rows of up to 128 bytes; the other warps only compute distances.
+template <int G, int DEGW, int LW, int H = 0>
+__global__ void __launch_bounds__(H ? 32 * (H + 1) : 160, 4)
+    batch_search_kernel(SearchArgs a, ReplayArgs ra) {
+    static_assert(H == 0 || (32 / G) * (H + 1) == 32, "helpers split 32 candidates");
     using namespace heapops;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
+    const int warp = H ? 0 : (int)(threadIdx.x >> 5);  // the warp's search area
+    const int hw = (int)(threadIdx.x >> 5);            // H > 0: 0 searches, others help
     const uint32_t dim = a.dim;
     const uint32_t dpad = (dim + 15u) & ~15u;
     float* pmin = reinterpret_cast<float*>(smem);
@@ -153,7 +167,7 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
     uint2* sps = reinterpret_cast<uint2*>(cd + kMaxDeg);
     float* ad = reinterpret_cast<float*>(sps + ra.scap);  // sorted pool: distances
     uint32_t* ai = reinterpret_cast<uint32_t*>(ad + acap);  // and ids
-    const size_t gw = (size_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    const size_t gw = (size_t)blockIdx.x * (H ? 1u : (blockDim.x >> 5)) + warp;
     const HeapView sp{sps, ra.sp_global + gw * ra.gcap, ra.scap};
     const uint32_t sp_max = ra.scap + ra.gcap;
 
@@ -167,6 +181,36 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
     const uint32_t lt = lanemask_lt();
     const int64_t mlist = a.nlist ? (int64_t)*a.nlist : a.m;
     const float INF = CUDART_INF_F;
+    __shared__ uint32_t s_cmd;  // H > 0: candidates to evaluate, or kCtaStop
+    constexpr uint32_t kCtaThreads = 32u * (H + 1);
+    if constexpr (H > 0) {
+        if (hw > 0) {
+            for (;;) {
+                named_bar(1, kCtaThreads);
+                const uint32_t nc = s_cmd;
+                if (nc == kCtaStop) break;
+                for (uint32_t b = 0; b < nc; b += 32)
+                    eval_batch<G, 1, LW, 1>(a, cid, cd, b + (uint32_t)hw * (32 / G), nc, qs, pmin,
+                                            pscale, g, r);
+                named_bar(2, kCtaThreads);
+            }
+            return;
+        }
+    }
+    // distances of cid[0, nc) into cd: this warp alone, or split over the block
+    auto eval_all = [&](uint32_t nc) {
+        if constexpr (H > 0) {
+            if (lane == 0) s_cmd = nc;
+            __syncwarp();
+            named_bar(1, kCtaThreads);
+            for (uint32_t b = 0; b < nc; b += 32)
+                eval_batch<G, 1, LW, 1>(a, cid, cd, b, nc, qs, pmin, pscale, g, r);
+            named_bar(2, kCtaThreads);
+        } else {
+            for (uint32_t b = 0; b < nc; b += 32)
+                eval_batch<G, G, LW, 1>(a, cid, cd, b, nc, qs, pmin, pscale, g, r);
+        }
+    };
 
     for (;;) {
         uint32_t slot = 0;
@@ -186,7 +230,10 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
         const uint32_t ep = a.entry;
         if (lane == 0) cid[0] = ep;
         __syncwarp();
-        eval_batch<G, G, LW, 1>(a, cid, cd, 0, 1, qs, pmin, pscale, g, r);
+        if constexpr (H > 0)
+            eval_batch<G, 1, LW, 1>(a, cid, cd, 0, 1, qs, pmin, pscale, g, r);
+        else
+            eval_batch<G, G, LW, 1>(a, cid, cd, 0, 1, qs, pmin, pscale, g, r);
         __syncwarp();
         const float d0 = cd[0];
         bool fail = !(d0 < INF);
@@ -293,8 +340,15 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
             }
 
             // qg.hpp:325-328
-            for (uint32_t b = 0; b < ncand; b += 32)
-                eval_batch<G, G, LW, 1>(a, cid, cd, b, ncand, qs, pmin, pscale, g, r);
+            if constexpr (H > 0) {
+                // the next pop is the first unpopped pool entry or an accepted
+                // candidate of this expansion: ask L2 for the pool entry's list
+                // while the distances are computed
+                if (cur < alen && lane == 0)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.nbrs + (size_t)(ai[cur] & ~kPopped) *
+                                                                         a.deg));
+            }
+            eval_all(ncand);
             calcs += ncand;
             __syncwarp();
 
@@ -481,19 +535,35 @@ __global__ void __launch_bounds__(160, 4) batch_search_kernel(SearchArgs a, Repl
         }
         __syncwarp();
     }
+    if constexpr (H > 0) {
+        if (lane == 0) s_cmd = kCtaStop;
+        __syncwarp();
+        named_bar(1, kCtaThreads);
+    }
 }
 
-template <int G, int DEGW, int LW>
+template <int G, int DEGW, int LW, int H = 0>
 static cudaError_t batch_run(const SearchArgs& a, const ReplayArgs& ra, int warps, int blocks,
                             cudaStream_t st, int* occ) {
     const size_t dpad = (a.dim + 15u) & ~15u;
-    const size_t smem = 8 * dpad + (size_t)warps * batch_warp_bytes(a.dim, a.vbits, ra.scap, ra.acap);
-    auto k = batch_search_kernel<G, DEGW, LW>;
+    const int areas = H ? 1 : warps;
+    const int threads = H ? 32 * (H + 1) : warps * 32;
+    const size_t smem = 8 * dpad + (size_t)areas * batch_warp_bytes(a.dim, a.vbits, ra.scap, ra.acap);
+    auto k = batch_search_kernel<G, DEGW, LW, H>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, warps * 32, smem);
-    k<<<blocks, warps * 32, smem, st>>>(a, ra);
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, threads, smem);
+    k<<<blocks, threads, smem, st>>>(a, ra);
     return cudaGetLastError();
+}
+
+// The query-per-block form: 4 lanes per candidate, 4 warps (8 candidates
+// each); a lane holds one code word per 16-dimension chunk, so 16 words in
+// flight cover 8 chunks per round.
+template <int DEGW>
+cudaError_t batch_cta_run(const SearchArgs& a, const ReplayArgs& ra, int blocks, cudaStream_t st,
+                          int* occ) {
+    return batch_run<4, DEGW, 16, 3>(a, ra, 1, blocks, st, occ);
 }
 
 // All instances for one lanes-per-candidate G: degree words 1-4, each with

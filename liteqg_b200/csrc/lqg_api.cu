@@ -249,7 +249,21 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         SearchArgs h = base_args(ix, w, b);
         h.qhead = w.d_ctl + kCtlHeapHead;
         h.vbits = t.visited_bits;
+        // small batches: one query per block of 4 warps, when every query of
+        // the batch can be resident at once
+        bool cta = false;
+        if (batch && t.small_batch != LQG_SMALL_BATCH_OFF &&
+            lqg::batch_smem_bytes(ix->dim, t.visited_bits, ra.scap, ra.acap, 1) <= 227 * 1024) {
+            int oc = 0;
+            e = lqg::launch_batch_cta(h, ra, degw, 0, b.st, &oc);
+            if (e != cudaSuccess) return cuda_fail(e, "small-batch kernel occupancy");
+            const int64_t lim =
+                t.small_batch == LQG_SMALL_BATCH_AUTO ? (int64_t)oc * ix->num_sms : t.small_batch;
+            cta = oc > 0 && b.m <= lim;
+        }
+        if (cta) sw = 1;
         auto launch = [&](const SearchArgs& c, int blocks, int* occ) {
+            if (cta) return lqg::launch_batch_cta(c, ra, degw, blocks, b.st, occ);
             if (batch)
                 return lqg::launch_batch(c, ra, (int)t.lanes_per_cand, degw, sw, blocks, b.st, occ);
             return split ? lqg::launch_split(c, ra, RE, (int)t.lanes_per_cand, degw, sw, blocks, b.st, occ)
@@ -762,6 +776,7 @@ lqg_status lqg_set_tuning(lqg_index* ix, const lqg_tuning* t) {
         n.heap_scap = t->heap_scap;
     }
     n.replay_all = t->replay_all ? 1u : 0u;
+    if (t->small_batch) n.small_batch = t->small_batch;
     if (t->replay_warps) {
         if (t->replay_warps > 15) return fail(LQG_ERR_ARG, "replay_warps must be in [1, 15]");
         n.replay_warps = t->replay_warps;

@@ -204,7 +204,7 @@ struct lqg_index {
     cudaStream_t own_stream = nullptr;
     // default: the batch kernel with the lazy search heap (mode 6), the
     // fastest on the bench batch and for single queries
-    lqg_tuning tune{2, 10, 8, 0, 6, 4, 256, 15, 0};
+    lqg_tuning tune{2, 10, 8, 0, 6, 4, 256, 15, 0, LQG_SMALL_BATCH_AUTO};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // recorded around the fast kernel
 
     ~lqg_index() {

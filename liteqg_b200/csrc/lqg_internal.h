@@ -90,6 +90,11 @@ size_t batch_smem_bytes(uint32_t dim, uint32_t vbits, uint32_t scap, uint32_t ac
 bool batch_replays_in_place_host(uint32_t vbits, uint32_t scap, uint32_t acap, uint32_t rcap);
 cudaError_t launch_batch(const SearchArgs& a, const ReplayArgs& ra, int G, int degw, int warps,
                          int blocks, cudaStream_t st, int* occ);
+// Its query-per-block form (batch_cta.cu): one query per block of 4 warps,
+// each expansion's distances split over the warps; for batches smaller than
+// the GPU's resident warps, where a query's latency sets the batch time.
+cudaError_t launch_batch_cta(const SearchArgs& a, const ReplayArgs& ra, int degw, int blocks,
+                             cudaStream_t st, int* occ);
 // Result-heap replay pass over a[0, m): one warp per query.
 cudaError_t launch_rp_replay(const SearchArgs& a, const ReplayArgs& ra, cudaStream_t st);
 

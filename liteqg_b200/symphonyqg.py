@@ -202,9 +202,12 @@ class Index:
 
     def set_tuning(self, lanes_per_cand=0, visited_bits=0, warps_per_block=0,
                    blocks_per_sm=0, mode=0, heap_warps=0, heap_scap=0,
-                   replay_warps=0, replay_all=0) -> None:
+                   replay_warps=0, replay_all=0, small_batch=0) -> None:
+        """Launch shape (lqg_set_tuning; 0 keeps a field). small_batch: batches
+        of at most this many queries run one query per block of 4 warps
+        (_capi.SMALL_BATCH_AUTO: as many as fit at once; SMALL_BATCH_OFF: never)."""
         t = Tuning(lanes_per_cand, visited_bits, warps_per_block, blocks_per_sm, mode,
-                   heap_warps, heap_scap, replay_warps, replay_all)
+                   heap_warps, heap_scap, replay_warps, replay_all, small_batch)
         check(lib().lqg_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:

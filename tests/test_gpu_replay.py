@@ -31,12 +31,18 @@ def lqg():
     return liteqg_b200
 
 
-# (tuning mode, replay_all): the split kernel writes unambiguous outputs from
-# its sorted array; replay_all=1 sends every query through the checked result
-# replay pass instead, so both paths are covered.
-@pytest.fixture(params=[(3, 0), (4, 0), (4, 1), (5, 0), (5, 1), (6, 0), (6, 1)],
+OFF = 0xFFFFFFFF  # small_batch: never the query-per-block form
+
+
+# (tuning mode, replay_all[, small_batch]): the split kernel writes unambiguous
+# outputs from its sorted array; replay_all=1 sends every query through the
+# checked result replay pass instead, so both paths are covered. Batches of
+# these sizes run the batch kernels' query-per-block form (4 warps per query)
+# unless small_batch is OFF, which keeps one warp per query.
+@pytest.fixture(params=[(3, 0), (4, 0), (4, 1), (5, 0), (5, 1), (5, 0, OFF), (6, 0), (6, 1),
+                        (6, 0, OFF), (6, 1, OFF)],
                 ids=["replay", "split", "split-replay-all", "batch", "batch-replay-all",
-                     "lazy", "lazy-replay-all"])
+                     "batch-warp", "lazy", "lazy-replay-all", "lazy-warp", "lazy-warp-replay-all"])
 def mode(request):
     return request.param
 
@@ -44,7 +50,8 @@ def mode(request):
 def open_index(lqg, g, mode, **tune):
     ix = lqg.Index("QG", "L2", g["n"], g["dim"], g["deg"])
     ix.load(g["path"])
-    ix.set_tuning(mode=mode[0], replay_all=mode[1], **tune)
+    ix.set_tuning(mode=mode[0], replay_all=mode[1], small_batch=mode[2] if len(mode) > 2 else 0,
+                  **tune)
     return ix
 
 
@@ -164,7 +171,7 @@ def test_replay_larger_index_uneven_batch(lqg, tmp_path, mode, dim, deg, integer
     write_index(path, arr)
     ix = lqg.Index("QG", "L2", n, dim, deg)
     ix.load(path)
-    ix.set_tuning(mode=mode[0], replay_all=mode[1])
+    ix.set_tuning(mode=mode[0], replay_all=mode[1], small_batch=mode[2] if len(mode) > 2 else 0)
     o = Oracle(arr)
     q = gen(400)
     efq = rng.choice([1, 7, 32, 64, 100, 256, 512], size=len(q)).astype(np.uint32)
@@ -254,14 +261,16 @@ def test_repeated_ids_across_list_words(lqg, tmp_path, fix_mode):
         assert np.array_equal(st[:, 0], want.pops), ef
 
 
-@pytest.mark.parametrize("hd_mode", [2, 4, 5, 6])
-def test_high_dimension_degree_64_uneven_batch(lqg, tmp_path, hd_mode):
+@pytest.mark.parametrize("hd_mode,small", [(2, 0), (4, 0), (5, 0), (6, 0), (6, OFF)])
+def test_high_dimension_degree_64_uneven_batch(lqg, tmp_path, hd_mode, small):
     """The uneven high-dimension workload's shape at 12k nodes: D = 960
     (960-byte code rows, the long code-load window), degree 64, a float
     Gaussian mixture (centres N(0, 1), sigma 0.3), an exact-kNN graph, and one
     batch with per-query ef up to 512 and k in {1, 10, 100}: ids, pops and
     FP32 pools equal the oracle's in the heap kernel (mode 2, the tuner's
-    choice there), the split kernel (4) and the batch kernels (5, 6)."""
+    choice there), the split kernel (4) and the batch kernels (5, 6; 300
+    queries run one query per block of 4 warps, and with small_batch OFF one
+    per warp)."""
     from oracle.oracle import sq8_quantize
 
     rng = np.random.default_rng(960)
@@ -275,7 +284,7 @@ def test_high_dimension_degree_64_uneven_batch(lqg, tmp_path, hd_mode):
     write_index(path, arr)
     ix = lqg.Index("QG", "L2", n, dim, deg)
     ix.load(path)
-    ix.set_tuning(mode=hd_mode, lanes_per_cand=2, heap_scap=512)
+    ix.set_tuning(mode=hd_mode, lanes_per_cand=2, heap_scap=512, small_batch=small)
     o = Oracle(arr)
     q = gen(300)
     efq = rng.choice([32, 64, 128, 256, 512], size=len(q)).astype(np.uint32)
