@@ -1028,18 +1028,25 @@ def uneven_arm(args, w, name, device):
                          ef_ptr=e_dev.data_ptr(), k_ptr=k_dev.data_ptr(), stream=sh)
 
     best = None
-    # (mode, lanes per candidate, heap warps per block, heap slots, visited bits)
+    # (mode, lanes per candidate, heap warps per block, heap slots, visited
+    # bits[, 1: batch kernels one query per block of 4 warps])
     shapes = ((6, 2, 4, 512, 10), (6, 4, 4, 512, 10), (5, 2, 4, 512, 10), (4, 4, 4, 512, 10),
               (2, 2, 4, 512, 10), (2, 4, 4, 512, 10), (1, 4, 4, 512, 10),
               (2, 2, 4, 256, 10), (2, 2, 4, 256, 9), (2, 2, 2, 512, 10), (2, 2, 8, 256, 9),
               # larger visited caches: fewer forgotten nodes evaluated again at
               # ef up to 512, against fewer resident warps
-              (2, 2, 2, 512, 12), (2, 2, 4, 256, 11), (2, 2, 2, 256, 13), (2, 2, 3, 512, 12))
-    from liteqg_b200._capi import LqgError
+              (2, 2, 2, 512, 12), (2, 2, 4, 256, 11), (2, 2, 2, 256, 13), (2, 2, 3, 512, 12),
+              # the query-per-block form on the whole batch: 960-byte rows make
+              # the distances most of a pop, which its 4 warps share
+              (6, 4, 4, 512, 10, 1), (6, 4, 4, 512, 11, 1), (6, 4, 4, 512, 12, 1),
+              (5, 4, 4, 512, 11, 1))
+    from liteqg_b200._capi import SMALL_BATCH_AUTO, LqgError
 
     for shape in shapes:
-        mode, g, hw, scap, vb = shape
-        ix.set_tuning(mode=mode, lanes_per_cand=g, heap_warps=hw, heap_scap=scap, visited_bits=vb)
+        mode, g, hw, scap, vb = shape[:5]
+        cta = len(shape) > 5 and shape[5]
+        ix.set_tuning(mode=mode, lanes_per_cand=g, heap_warps=hw, heap_scap=scap, visited_bits=vb,
+                      small_batch=nq if cta else SMALL_BATCH_AUTO)
         try:
             for _ in range(2):
                 step()
@@ -1048,12 +1055,15 @@ def uneven_arm(args, w, name, device):
             log(f"[uneven] shape {shape} skipped: {e}")
             continue
         ms = _timed(step, 5, flush, stream)
-        log(f"[uneven] mode {mode} G {g} warps {hw} scap {scap} vbits {vb}: {ms:.2f} ms")
+        log(f"[uneven] mode {mode} G {g} warps {hw} scap {scap} vbits {vb} "
+            f"{'block per query ' if cta else ''}: {ms:.2f} ms")
         if best is None or ms < best[0]:
             best = (ms, shape)
-    mode, g, hw, scap, vb = best[1]
-    best = (best[0], mode, g)
-    ix.set_tuning(mode=mode, lanes_per_cand=g, heap_warps=hw, heap_scap=scap, visited_bits=vb)
+    mode, g, hw, scap, vb = best[1][:5]
+    cta = len(best[1]) > 5 and best[1][5]
+    best = (best[0], mode, g, hw, scap, vb, bool(cta))
+    ix.set_tuning(mode=mode, lanes_per_cand=g, heap_warps=hw, heap_scap=scap, visited_bits=vb,
+                  small_batch=nq if cta else SMALL_BATCH_AUTO)
     for _ in range(max(3, args.warmup)):
         step()
     ix.stream_status(sh)
@@ -1156,7 +1166,9 @@ def uneven_arm(args, w, name, device):
                                f"per-query ef from {list(w['ef_choices'])}, k from "
                                f"{list(w['k_choices'])} (seed 2)",
                    "recall_at_10_pool_by_ef": rec_by_ef, "pool_coverage_at_10_by_ef": cov_by_ef,
-                   "mode": best[1], "lanes_per_cand": best[2],
+                   "mode": best[1], "lanes_per_cand": 4 if best[6] else best[2],
+                   "warps_per_block": 4 if best[6] else best[3], "heap_scap": best[4],
+                   "visited_bits": best[5], "query_per_block": best[6],
                    "l2": "flushed between steps (256 MiB write)"},
         "graph_qps": nq / (graph_ms / 1e3), "graph_ids_equal": graph_ok,
         "gpu_launches": (5 + {1: 3, 2: 2, 3: 3, 4: 2, 5: 2, 6: 2}.get(best[1], 3)) * K,
@@ -1167,7 +1179,8 @@ def uneven_arm(args, w, name, device):
                      "kernel": {1: "fast_search_kernel + heap_search_kernel (tied queries)",
                                 2: "heap_search_kernel", 4: "split_search_kernel",
                                 5: "batch_search_kernel",
-                                6: "batch_search_kernel (lazy search heap)"}.get(best[1])},
+                                6: "batch_search_kernel (lazy search heap)"}.get(best[1]) +
+                               (", one query per block of 4 warps" if best[6] else "")},
         "e2e": {"value": e2e_qps, "unit": "queries/s",
                 "h2d_bytes_per_step": int(nq * dim * 4 + 8 * nq),
                 "d2h_bytes_per_step": int(nq * kmax * 4), "ids_equal": e2e_ok},

@@ -252,7 +252,7 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         // small batches: one query per block of 4 warps, when every query of
         // the batch can be resident at once
         bool cta = false;
-        if (batch && t.small_batch != LQG_SMALL_BATCH_OFF &&
+        if (batch && b.small_ok && t.small_batch != LQG_SMALL_BATCH_OFF &&
             lqg::batch_smem_bytes(ix->dim, t.visited_bits, ra.scap, ra.acap, 1) <= 227 * 1024) {
             int oc = 0;
             e = lqg::launch_batch_cta(h, ra, degw, 0, b.st, &oc);

@@ -137,6 +137,10 @@ struct BatchSpec {
     uint32_t ties_ok = 0;
     uint32_t* path = nullptr;  // index build: popped ids per query (fast kernel)
     uint32_t path_stride = 0;
+    // the query-per-block form may run (modes 5-6, small batches): false when
+    // other batches share the device, where its idle helper warps would cost
+    // throughput
+    bool small_ok = true;
 };
 
 template <typename T>

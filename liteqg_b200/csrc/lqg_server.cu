@@ -142,6 +142,7 @@ void dispatch_loop(lqg_server* s) {
     const uint32_t dim = s->ix->dim;
     for (;;) {
         Ctx* c = nullptr;
+        bool alone = false;  // no other batch in flight when this one launches
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] {
@@ -181,6 +182,9 @@ void dispatch_loop(lqg_server* s) {
                 rest.pop_back();
             }
             c->busy = true;
+            alone = true;
+            for (auto& x : s->ctx)
+                if (&x != c && x.busy) alone = false;
         }
         const uint32_t m = (uint32_t)c->batch.size();
         uint32_t efmax = 1;
@@ -201,6 +205,10 @@ void dispatch_loop(lqg_server* s) {
         if (st == LQG_OK) {
             BatchSpec b{c->d_q, (int64_t)m, c->d_k, 0, c->d_ef, efmax, c->d_ids,
                         s->cfg.max_k, nullptr, nullptr, 0, nullptr, c->st};
+            // a batch that has the device to itself may run one query per
+            // block (lower latency); under load the one-warp form keeps the
+            // throughput
+            b.small_ok = alone;
             st = run_batch(s->ix, c->ws, b, false);
         }
         if (st == LQG_OK) {
@@ -287,6 +295,7 @@ lqg_status warm_context(lqg_server* s, Ctx& c) {
         LQG_CUDA(cudaMemcpyAsync(c.d_ef, c.h_ef, (size_t)mb * 4, cudaMemcpyHostToDevice, c.st));
         BatchSpec b{c.d_q, (int64_t)mb, c.d_k, 0, c.d_ef, s->class_ef[ci], c.d_ids,
                     s->cfg.max_k, nullptr, nullptr, 0, nullptr, c.st};
+        b.small_ok = false;  // the one-warp form's work areas are the larger
         const lqg_status st = run_batch(s->ix, c.ws, b, false);
         if (st != LQG_OK) return st;
         LQG_CUDA(cudaStreamSynchronize(c.st));
