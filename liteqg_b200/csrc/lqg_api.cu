@@ -254,12 +254,17 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
         bool cta = false;
         if (batch && b.small_ok && t.small_batch != LQG_SMALL_BATCH_OFF &&
             lqg::batch_smem_bytes(ix->dim, t.visited_bits, ra.scap, ra.acap, 1) <= 227 * 1024) {
-            int oc = 0;
-            e = lqg::launch_batch_cta(h, ra, degw, 0, b.st, &oc);
-            if (e != cudaSuccess) return cuda_fail(e, "small-batch kernel occupancy");
-            const int64_t lim =
-                t.small_batch == LQG_SMALL_BATCH_AUTO ? (int64_t)oc * ix->num_sms : t.small_batch;
-            cta = oc > 0 && b.m <= lim;
+            if (plain) {
+                cta = true;  // one query: no occupancy question
+            } else {
+                int oc = 0;
+                e = lqg::launch_batch_cta(h, ra, degw, 0, b.st, &oc);
+                if (e != cudaSuccess) return cuda_fail(e, "small-batch kernel occupancy");
+                const int64_t lim = t.small_batch == LQG_SMALL_BATCH_AUTO
+                                        ? (int64_t)oc * ix->num_sms
+                                        : t.small_batch;
+                cta = oc > 0 && b.m <= lim;
+            }
         }
         if (cta) sw = 1;
         auto launch = [&](const SearchArgs& c, int blocks, int* occ) {
@@ -432,10 +437,8 @@ lqg_status run_batch(lqg_index* ix, Workspace& w, BatchSpec& b, bool plain) {
     return LQG_OK;
 }
 
-lqg_status read_status(Workspace& w, cudaStream_t st) {
-    uint32_t ctl[kCtlWords];
-    LQG_CUDA(cudaMemcpyAsync(ctl, w.d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
-    LQG_CUDA(cudaStreamSynchronize(st));
+// The status of a finished batch from its control words.
+lqg_status status_of(const uint32_t* ctl) {
     if (ctl[kCtlErr]) {
         std::string why;
         if (ctl[kCtlErr] & lqg::kErrVisitedFull) why += " visited set full (32768 nodes);";
@@ -447,6 +450,13 @@ lqg_status read_status(Workspace& w, cudaStream_t st) {
                                           std::to_string(ctl[kCtlErrQuery]) + ":" + why);
     }
     return LQG_OK;
+}
+
+lqg_status read_status(Workspace& w, cudaStream_t st) {
+    uint32_t ctl[kCtlWords];
+    LQG_CUDA(cudaMemcpyAsync(ctl, w.d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
+    LQG_CUDA(cudaStreamSynchronize(st));
+    return status_of(ctl);
 }
 
 // Host-buffer batch: copy in, search, copy out, wait (one workspace).
@@ -662,11 +672,33 @@ lqg_status lqg_search(lqg_index* ix, const float* query, uint32_t k, uint32_t* r
     if ((s = grow(w.d_q, w.cap_q, ix->dim)) != LQG_OK) return s;
     if ((s = grow(w.d_ids, w.cap_ids, k)) != LQG_OK) return s;
     cudaStream_t st = ix->own_stream;
-    LQG_CUDA(cudaMemcpyAsync(w.d_q, query, ix->dim * 4, cudaMemcpyHostToDevice, st));
+    // pinned staging: query | ids | control words, each on 16 bytes
+    const size_t qb = ((size_t)ix->dim * 4 + 15) & ~(size_t)15;
+    const size_t ib = ((size_t)k * 4 + 15) & ~(size_t)15;
+    const size_t need = qb + ib + kCtlWords * sizeof(uint32_t);
+    if (w.cap_h_plain < need) {
+        if (w.h_plain) cudaFreeHost(w.h_plain);
+        w.h_plain = nullptr;
+        w.cap_h_plain = 0;
+        if (cudaHostAlloc(&w.h_plain, need, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LQG_ERR_NOMEM, "pinned staging allocation failed");
+        }
+        w.cap_h_plain = need;
+    }
+    float* h_q = reinterpret_cast<float*>(w.h_plain);
+    uint32_t* h_ids = reinterpret_cast<uint32_t*>(w.h_plain + qb);
+    uint32_t* h_ctl = reinterpret_cast<uint32_t*>(w.h_plain + qb + ib);
+    std::memcpy(h_q, query, (size_t)ix->dim * 4);
+    LQG_CUDA(cudaMemcpyAsync(w.d_q, h_q, ix->dim * 4, cudaMemcpyHostToDevice, st));
     BatchSpec b{w.d_q, 1, nullptr, k, nullptr, 0, w.d_ids, k, nullptr, nullptr, 0, nullptr, st};
     if ((s = run_batch(ix, w, b, true)) != LQG_OK) return s;
-    LQG_CUDA(cudaMemcpyAsync(results, w.d_ids, k * 4, cudaMemcpyDeviceToHost, st));
-    return read_status(w, st);
+    LQG_CUDA(cudaMemcpyAsync(h_ids, w.d_ids, k * 4, cudaMemcpyDeviceToHost, st));
+    LQG_CUDA(cudaMemcpyAsync(h_ctl, w.d_ctl, kCtlWords * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                             st));
+    LQG_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(results, h_ids, (size_t)k * 4);
+    return status_of(h_ctl);
 }
 
 lqg_status lqg_search_batch_device(lqg_index* ix, const float* queries, int64_t m,

@@ -78,7 +78,15 @@ struct Workspace {
     uint32_t* d_stats = nullptr;
     size_t cap_q = 0, cap_kq = 0, cap_efq = 0, cap_ids = 0, cap_pool_ids = 0, cap_pool_d = 0,
            cap_stats = 0;
+    // one-query calls: pinned host staging for the query, the ids and the
+    // control words, so the copies are plain DMA and one synchronisation ends
+    // the call
+    unsigned char* h_plain = nullptr;
+    size_t cap_h_plain = 0;
     void release() {
+        if (h_plain) cudaFreeHost(h_plain);
+        h_plain = nullptr;
+        cap_h_plain = 0;
         dfree(d_ctl);
         dfree(d_flagged);
         dfree(d_spill);
