@@ -294,7 +294,7 @@ typedef struct {
     uint64_t completed;    /* requests finished since start / reset */
     uint64_t batches;
     double mean_batch;
-    double p50_us, p99_us; /* latency submit -> result */
+    double p50_us, p99_us; /* latency arrival -> result */
     double qps;            /* completed / elapsed */
     uint32_t max_batch, streams;  /* max_batch: the largest class's count */
 } lqg_server_metrics;
@@ -308,8 +308,9 @@ LQG_API lqg_status lqg_server_submit(lqg_server* s, const float* query, uint32_t
 LQG_API lqg_status lqg_server_wait(lqg_server* s, uint64_t ticket, uint32_t* ids,
                                    int64_t timeout_us, double* latency_us);
 /* Open-loop driver: submits query i at arrival_us[i] (from the call's start;
- * NULL = as fast as possible) from a client thread, waits for all; ids
- * [m][kstride], latency_us [m] (may be NULL). */
+ * NULL = as fast as possible) from a client thread (all requests already due
+ * in one step), waits for all; ids [m][kstride], latency_us [m] (may be
+ * NULL), measured from each request's scheduled arrival. */
 LQG_API lqg_status lqg_server_replay(lqg_server* s, const float* queries, int64_t m,
                                      const uint32_t* k, const uint32_t* ef,
                                      const double* arrival_us, uint32_t* ids,

@@ -19,8 +19,9 @@
 // share of the device budget. An ef-50 request therefore reserves an ef-64
 // footprint, not an ef-512 one, and short requests are not held behind long
 // ones of a larger class. A completer thread waits for batches in launch
-// order, hands each request its ids and records its latency
-// (submit -> result).
+// order, hands each request its ids and records its latency (arrival ->
+// result; in lqg_server_replay the arrival is the scheduled one, so a client
+// that falls behind its schedule shows in the latency).
 //
 // Each request is searched by the same kernels and with its own k and ef, so
 // its result is exactly what a batched or single search of that query alone
@@ -51,7 +52,9 @@ struct Request {
     uint32_t k = 0, ef = 0;
     std::vector<float> q;
     std::vector<uint32_t> ids;
-    Clock::time_point t_submit, t_done;
+    // t_arrive: when the request arrived (the submit call, or its scheduled
+    // arrival in lqg_server_replay); latency is measured from it
+    Clock::time_point t_arrive, t_done;
     lqg_status status = LQG_OK;
     bool done = false;
 };
@@ -248,16 +251,21 @@ void complete_loop(lqg_server* s) {
             st = fail(LQG_ERR_CUDA, "batch failed on the device");
         if (st == LQG_OK && c->h_ctl[kCtlErr]) st = LQG_ERR_CAPACITY;
         const auto now = Clock::now();
+        // the batch's requests belong to this context until marked done: their
+        // ids are copied outside the lock the submitters and waiters share
+        for (size_t i = 0; i < c->batch.size(); ++i) {
+            Request* r = c->batch[i];
+            r->ids.assign(c->h_ids + i * s->cfg.max_k, c->h_ids + i * s->cfg.max_k + r->k);
+            r->status = st;
+            r->t_done = now;
+        }
         {
             std::lock_guard<std::mutex> lk(s->mu);
             for (size_t i = 0; i < c->batch.size(); ++i) {
                 Request* r = c->batch[i];
-                r->ids.assign(c->h_ids + i * s->cfg.max_k, c->h_ids + i * s->cfg.max_k + r->k);
-                r->status = st;
-                r->t_done = now;
                 r->done = true;
                 s->lat_us.push_back(
-                    std::chrono::duration<double, std::micro>(now - r->t_submit).count());
+                    std::chrono::duration<double, std::micro>(now - r->t_arrive).count());
                 ++s->completed;
             }
             c->batch.clear();
@@ -388,7 +396,7 @@ lqg_status lqg_server_submit(lqg_server* s, const float* query, uint32_t k, uint
     r->k = k;
     r->ef = ef;
     r->q.assign(query, query + s->ix->dim);
-    r->t_submit = Clock::now();
+    r->t_arrive = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stopping) {
@@ -418,7 +426,7 @@ lqg_status lqg_server_wait(lqg_server* s, uint64_t ticket, uint32_t* ids, int64_
         return fail(LQG_ERR_STATE, "timed out");
     }
     if (ids) std::memcpy(ids, r->ids.data(), r->ids.size() * 4);
-    if (latency_us) *latency_us = std::chrono::duration<double, std::micro>(r->t_done - r->t_submit).count();
+    if (latency_us) *latency_us = std::chrono::duration<double, std::micro>(r->t_done - r->t_arrive).count();
     lqg_status st = r->status;
     s->reqs.erase(it);
     delete r;
@@ -435,22 +443,74 @@ lqg_status lqg_server_replay(lqg_server* s, const float* queries, int64_t m, con
     for (auto& t : tickets) t.store(0);
     std::atomic<int> err{LQG_OK};
     std::atomic<int64_t> submitted{0};
+    // the client submits, under one lock, every request whose arrival time
+    // has come (up to 1,024 at once), and stamps each with its scheduled
+    // arrival, so a client that falls behind shows as latency, not as a lower
+    // offered rate
     std::thread client([&] {
         const auto t0 = Clock::now();
-        for (int64_t i = 0; i < m; ++i) {
+        auto due_of = [&](int64_t i) {
+            return t0 + std::chrono::duration_cast<Clock::duration>(
+                            std::chrono::duration<double, std::micro>(arrival_us[i]));
+        };
+        std::vector<Request*> group;
+        int64_t i = 0;
+        while (i < m) {
             if (arrival_us) {
-                const auto due = t0 + std::chrono::duration_cast<Clock::duration>(
-                                          std::chrono::duration<double, std::micro>(arrival_us[i]));
+                const auto due = due_of(i);
                 while (Clock::now() < due) {
                     const auto left = due - Clock::now();
                     if (left > std::chrono::microseconds(200)) std::this_thread::sleep_for(left / 2);
                 }
             }
-            uint64_t t = 0;
-            lqg_status st = lqg_server_submit(s, queries + (size_t)i * s->ix->dim, k[i], ef[i], &t);
-            if (st != LQG_OK) err.store(st);
-            tickets[(size_t)i].store(st == LQG_OK ? t : ~0ull);
-            submitted.store(i + 1);
+            const auto now = Clock::now();
+            int64_t j = i + 1;
+            if (arrival_us)
+                while (j < m && j - i < 1024 && due_of(j) <= now) ++j;
+            group.clear();
+            for (int64_t x = i; x < j; ++x) {
+                const uint32_t kx = k[x], efx = ef[x] ? ef[x] : s->ix->ef;
+                if (kx == 0 || kx > s->cfg.max_k || efx == 0 || efx > s->cfg.max_ef) {
+                    err.store(fail(LQG_ERR_ARG, "request k or ef out of range"));
+                    tickets[(size_t)x].store(~0ull);
+                    group.push_back(nullptr);
+                    continue;
+                }
+                auto* r = new (std::nothrow) Request();
+                if (!r) {
+                    err.store(fail(LQG_ERR_NOMEM, "host allocation failed"));
+                    tickets[(size_t)x].store(~0ull);
+                    group.push_back(nullptr);
+                    continue;
+                }
+                r->k = kx;
+                r->ef = efx;
+                r->q.assign(queries + (size_t)x * s->ix->dim, queries + (size_t)(x + 1) * s->ix->dim);
+                r->t_arrive = arrival_us ? due_of(x) : now;
+                group.push_back(r);
+            }
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                for (int64_t x = i; x < j; ++x) {
+                    Request* r = group[(size_t)(x - i)];
+                    if (!r) continue;
+                    if (s->stopping) {
+                        delete r;
+                        group[(size_t)(x - i)] = nullptr;
+                        err.store(fail(LQG_ERR_STATE, "server is stopping"));
+                        tickets[(size_t)x].store(~0ull);
+                        continue;
+                    }
+                    r->ticket = s->next_ticket++;
+                    s->reqs[r->ticket] = r;
+                    s->pending.push_back(r);
+                }
+            }
+            s->cv_work.notify_one();
+            for (int64_t x = i; x < j; ++x)
+                if (Request* r = group[(size_t)(x - i)]) tickets[(size_t)x].store(r->ticket);
+            submitted.store(j);
+            i = j;
         }
     });
     // collect in submission order (each wait blocks until that ticket exists and is done)
