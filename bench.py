@@ -535,6 +535,10 @@ def gpu_arm(args, w, name, rank, world, device):
         ix = liteqg_b200.Index("QG", "L2", n, dim, deg, device=device)
         ix.load(path)
         ef = args.ef or w["efs"][0]
+        if args.profile_queries:
+            # a smaller batch (e.g. one that runs one query per block)
+            queries = queries[:args.profile_queries]
+            nq = len(queries)
         c = FIXED_TUNING[args.mode or 6]
         ix.set_tuning(mode=c[0], lanes_per_cand=c[1], visited_bits=c[2], warps_per_block=c[3],
                       heap_warps=c[4], heap_scap=c[5])
@@ -1432,6 +1436,8 @@ def main():
     ap.add_argument("--build-only", action="store_true",
                     help="build the workload's index (no cache), print the build report, exit")
     ap.add_argument("--ef", type=int, default=0, help="--profile: the ef to search with")
+    ap.add_argument("--profile-queries", type=int, default=0,
+                    help="--profile: search only the first N queries per step")
     ap.add_argument("--fastscan", action="store_true",
                     help="--profile: run the FastScan/RaBitQ search instead of the SQ8 search")
     ap.add_argument("--prepare", action="store_true",
