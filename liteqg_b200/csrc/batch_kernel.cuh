@@ -129,7 +129,6 @@ __device__ __forceinline__ uint32_t upper_rank(const float* a, uint32_t n, float
 // words at a time needs dozens of dependent rounds, which costs more than the
 // spills.
 constexpr int batch_load_words(int degw) { return degw == 1 ? 16 : 8; }
-constexpr uint32_t kBatchWideDim = 256;
 
 // Named barriers of the query-per-block form (barrier 0 is __syncthreads).
 __device__ __forceinline__ void named_bar(uint32_t id, uint32_t threads) {

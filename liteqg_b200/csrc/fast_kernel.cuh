@@ -33,8 +33,15 @@
 
 #include "lqg_internal.h"
 #include "lqg_kernels.cuh"
+#include "sq8_batch.cuh"
 
 namespace lqg {
+
+// Code words in flight per lane in the fast kernel's distance batches: the
+// 512-entry pool (E = 16) holds 32 registers per lane, so it gets the short
+// window.
+template <int E>
+constexpr int kFastLoadWords = E >= 16 ? 8 : 16;
 
 template <int E>
 __device__ __forceinline__ float pool_at(const float (&pd)[E], uint32_t lane_of, uint32_t slot_of) {
@@ -156,14 +163,29 @@ __global__ void __launch_bounds__(512) fast_search_kernel(SearchArgs a) {
                 __syncwarp();
             }
 
-            // qg.hpp:325-328: SQ8 decode + L2 of every kept neighbour.
-            for (uint32_t base = 0; base < ncand; base += CPP) {
-                const uint32_t c = base + g;
-                const bool valid = c < ncand;
-                const uint32_t id = valid ? cid[c] : 0u;
-                const float d = sq8_l2_group<G>(a.codes + (size_t)id * a.cstride, valid, qs,
-                                                pmin, pscale, dim, r);
-                if (valid && r == 0) cd[c] = d;
+            // qg.hpp:325-328: SQ8 decode + L2 of every kept neighbour. Rows
+            // below 256 bytes with up to 4 lanes per candidate: the packed-pair
+            // batch routine (32 candidates per call, code loads of every pass
+            // issued before the arithmetic; the same operations in the same
+            // order). Longer rows, or wider groups: one candidate per group at
+            // a time with 8 chunks of the row in flight (the batch routine's
+            // short load window would take a dependent round per two chunks).
+            bool packed = false;
+            if constexpr (G <= 4) packed = dim < kBatchWideDim;
+            if (packed) {
+                if constexpr (G <= 4)
+                    for (uint32_t b = 0; b < ncand; b += 32)
+                        eval_batch<G, G, kFastLoadWords<E>, 1>(a, cid, cd, b, ncand, qs, pmin,
+                                                               pscale, g, r);
+            } else {
+                for (uint32_t base = 0; base < ncand; base += CPP) {
+                    const uint32_t c = base + g;
+                    const bool valid = c < ncand;
+                    const uint32_t id = valid ? cid[c] : 0u;
+                    const float d = sq8_l2_group<G>(a.codes + (size_t)id * a.cstride, valid, qs,
+                                                    pmin, pscale, dim, r);
+                    if (valid && r == 0) cd[c] = d;
+                }
             }
             calcs += ncand;
             __syncwarp();

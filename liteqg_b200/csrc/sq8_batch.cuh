@@ -12,6 +12,10 @@
 
 namespace lqg {
 
+// Rows of at least this many code bytes ("wide") need a longer code-load
+// window than narrow ones: the window is counted in 16-byte chunks per round.
+constexpr uint32_t kBatchWideDim = 256;
+
 // ---- packed FP32 pairs -----------------------------------------------------
 
 __device__ __forceinline__ unsigned long long pk(uint32_t lo, uint32_t hi) {
