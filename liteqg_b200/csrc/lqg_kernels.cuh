@@ -131,6 +131,31 @@ __device__ __forceinline__ void load_vec(const float* p, float (&v)[A]) {
     }
 }
 
+// ---- packed FP32 pairs -----------------------------------------------------
+
+__device__ __forceinline__ unsigned long long pk(uint32_t lo, uint32_t hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(lo), "r"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk(unsigned long long v, float& lo, float& hi) {
+    uint32_t a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(a), "=r"(b) : "l"(v));
+    lo = __uint_as_float(a);
+    hi = __uint_as_float(b);
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
 // Squared L2 between the query (shared memory, qs) and the SQ8-decoded row.
 // Called by all 32 lanes together; lane r = lane % G of each group handles
 // accumulators [r*A, r*A + A). `valid` lanes load; the others compute on
@@ -151,6 +176,13 @@ __device__ __forceinline__ float sq8_l2_group(const uint8_t* row, bool valid,
     // Up to U chunks of the row are requested before any arithmetic, so the
     // global-memory latency is paid once per U chunks, not once per chunk.
     constexpr int U = 8;
+    // A >= 2: the arithmetic on packed FP32 pairs (fma.rn.f32x2 and
+    // sub.rn.f32x2 round each half exactly as the scalar instructions do)
+    constexpr int AP = A >= 2 ? A / 2 : 1;
+    unsigned long long acc2[AP];
+#pragma unroll
+    for (int t = 0; t < AP; ++t) acc2[t] = 0ull;
+    const unsigned long long C23 = pk(0x4B000000u, 0x4B000000u);
     for (uint32_t base = 0; base < mul; base += 16 * U) {
         uint32_t w[U][W];
 #pragma unroll
@@ -167,19 +199,56 @@ __device__ __forceinline__ float sq8_l2_group(const uint8_t* row, bool valid,
         for (int u = 0; u < U; ++u) {
             const uint32_t d0 = base + 16 * u + r * A;
             if (base + 16 * u < mul) {
-                float qv[A], mv[A], sv[A];
-                load_vec<A>(qs + d0, qv);
-                load_vec<A>(pmin + d0, mv);
-                load_vec<A>(pscale + d0, sv);
+                if constexpr (A >= 2) {
+                    unsigned long long q2[AP], m2[AP], s2[AP];
+                    if constexpr (AP >= 2) {
 #pragma unroll
-                for (int t = 0; t < A; ++t) {
-                    float c = byte_to_float(w[u][t / 4], t % 4);
-                    float dec = __fmaf_rn(c, sv[t], mv[t]);
-                    float df = __fsub_rn(qv[t], dec);
-                    acc[t] = __fmaf_rn(df, df, acc[t]);
+                        for (int t = 0; t < AP; t += 2) {
+                            const ulonglong2 qq = *reinterpret_cast<const ulonglong2*>(qs + d0 + 2 * t);
+                            const ulonglong2 mm = *reinterpret_cast<const ulonglong2*>(pmin + d0 + 2 * t);
+                            const ulonglong2 ss = *reinterpret_cast<const ulonglong2*>(pscale + d0 + 2 * t);
+                            q2[t] = qq.x;
+                            q2[t + 1] = qq.y;
+                            m2[t] = mm.x;
+                            m2[t + 1] = mm.y;
+                            s2[t] = ss.x;
+                            s2[t + 1] = ss.y;
+                        }
+                    } else {
+                        q2[0] = *reinterpret_cast<const unsigned long long*>(qs + d0);
+                        m2[0] = *reinterpret_cast<const unsigned long long*>(pmin + d0);
+                        s2[0] = *reinterpret_cast<const unsigned long long*>(pscale + d0);
+                    }
+#pragma unroll
+                    for (int t = 0; t < AP; ++t) {
+                        const uint32_t wd = w[u][(2 * t) / 4];
+                        const int s0 = (2 * t) % 4;
+                        const uint32_t lo = __byte_perm(wd, 0x4B000000u, 0x7440u + s0);
+                        const uint32_t hi = __byte_perm(wd, 0x4B000000u, 0x7440u + s0 + 1);
+                        const unsigned long long c2 = sub2(pk(lo, hi), C23);
+                        const unsigned long long dec = fma2(c2, s2[t], m2[t]);
+                        const unsigned long long df = sub2(q2[t], dec);
+                        acc2[t] = fma2(df, df, acc2[t]);
+                    }
+                } else {
+                    float qv[A], mv[A], sv[A];
+                    load_vec<A>(qs + d0, qv);
+                    load_vec<A>(pmin + d0, mv);
+                    load_vec<A>(pscale + d0, sv);
+#pragma unroll
+                    for (int t = 0; t < A; ++t) {
+                        float c = byte_to_float(w[u][t / 4], t % 4);
+                        float dec = __fmaf_rn(c, sv[t], mv[t]);
+                        float df = __fsub_rn(qv[t], dec);
+                        acc[t] = __fmaf_rn(df, df, acc[t]);
+                    }
                 }
             }
         }
+    }
+    if constexpr (A >= 2) {
+#pragma unroll
+        for (int t = 0; t < AP; ++t) upk(acc2[t], acc[2 * t], acc[2 * t + 1]);
     }
     // fold tree: h = 8, 4, 2, 1
 #pragma unroll

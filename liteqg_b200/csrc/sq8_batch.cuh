@@ -16,31 +16,6 @@ namespace lqg {
 // window than narrow ones: the window is counted in 16-byte chunks per round.
 constexpr uint32_t kBatchWideDim = 256;
 
-// ---- packed FP32 pairs -----------------------------------------------------
-
-__device__ __forceinline__ unsigned long long pk(uint32_t lo, uint32_t hi) {
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(lo), "r"(hi));
-    return r;
-}
-__device__ __forceinline__ void upk(unsigned long long v, float& lo, float& hi) {
-    uint32_t a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=r"(a), "=r"(b) : "l"(v));
-    lo = __uint_as_float(a);
-    hi = __uint_as_float(b);
-}
-__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
-                                                   unsigned long long c) {
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
-    unsigned long long d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-
 // Distances of candidates cid[base + p * (32/G) + g], p < NP, into cd[].
 // Lane r of group g owns accumulators [r*A, r*A + A) (A = 16/G); all code
 // bytes of a round of U chunks, for all NP passes, are requested before any
