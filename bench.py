@@ -588,12 +588,15 @@ def gpu_arm(args, w, name, rank, world, device):
     ix.set_ef(chosen)
     log(f"[rank {rank}] ef={chosen} recall={recall} {time.perf_counter() - t0:.1f}s")
     knn_recall = None
+    ref_built = None
     if w.get("knn_compare") and rank == 0:
         # the same search on the exact deg-NN graph of the same data (same
         # entry point, codes and parameters): what the builder's candidate
         # cap and the reference's omitted refine round could at most give
         knn_recall = knn_graph_recall(ix, w, gen_data(w, "base"), queries, gt, device)
         log(f"[rank {rank}] exact-kNN-graph recall {knn_recall}")
+        ref_built = reference_built_recall(w, gen_data(w, "base"), queries, gt, device)
+        log(f"[rank {rank}] reference-built index recall {ref_built}")
 
     dev = torch.device("cuda", device)
     stream = torch.cuda.current_stream(dev)
@@ -765,6 +768,7 @@ def gpu_arm(args, w, name, rank, world, device):
         "config": {"workload": workload_str(name, w, nq, k, chosen), "ef": chosen, "k": k,
                    "recall_at_10_pool": recall.get(chosen), "recall_by_ef": recall,
                    **({"recall_by_ef_exact_knn_graph": knn_recall} if knn_recall else {}),
+                   **({"reference_built_index": ref_built} if ref_built else {}),
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                    "tuning": tune, "autotune_ms": mode_ms, "tied_query_share": exact_share,
                    "fast_vs_exact_id_mismatch": mismatch, "e2e_ids_equal": e2e_ok,
@@ -826,6 +830,45 @@ def knn_graph_recall(ix, w, base, queries, gt, device):
         out[ef] = recall_at(pid, gt, 10)
     kx.close()
     return out
+
+
+def reference_built_recall(w, base, queries, gt, device):
+    """Best-10-of-pool recall by ef of the same search (this package's, exact
+    against the reference) on an index built from the same base vectors by
+    the reference's own builder (QGBuilder, compiled from its sources into
+    oracle/_ref, on all host cores), and the build's wall time; None when
+    oracle/_ref is absent."""
+    import tempfile
+
+    import liteqg_b200
+    from oracle.oracle import RefHarness, ref_available
+
+    if not ref_available():
+        return None
+    path = os.path.join(tempfile.mkdtemp(), "reference_built.idx")
+    # the reference's builder prints its progress on stdout, which carries
+    # only this program's JSON line: point file descriptor 1 at stderr
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        t = time.perf_counter()
+        RefHarness().build(base, w["deg"], w["efb"], w["iters"], path,
+                           nthreads=os.cpu_count() or 1)
+        build_s = time.perf_counter() - t
+    finally:
+        C.CDLL(None).fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+    rx = liteqg_b200.Index("QG", "L2", w["n"], w["dim"], w["deg"], device=device)
+    rx.load(path)
+    out = {}
+    for ef in w["efs"]:
+        _, (pid, _) = rx.search(queries, 10, ef=ef, return_pool=True)
+        out[ef] = recall_at(pid, gt, 10)
+    rx.close()
+    os.remove(path)
+    return {"recall_by_ef": out, "build_s": build_s, "threads": os.cpu_count() or 1}
 
 
 def grid_points(ix, w, name, path, queries, q_dev, gt, flush, stream, peak):
