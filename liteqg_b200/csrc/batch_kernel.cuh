@@ -180,7 +180,8 @@ __global__ void __launch_bounds__(H ? 32 * (H + 1) : 160, 4)
     const uint32_t lt = lanemask_lt();
     const int64_t mlist = a.nlist ? (int64_t)*a.nlist : a.m;
     const float INF = CUDART_INF_F;
-    __shared__ uint32_t s_cmd;  // H > 0: candidates to evaluate, or kCtaStop
+    __shared__ uint32_t s_cmd;   // H > 0: candidates to evaluate, or kCtaStop
+    __shared__ uint32_t s_hint;  // H > 0: the first unpopped pool entry's id
     constexpr uint32_t kCtaThreads = 32u * (H + 1);
     if constexpr (H > 0) {
         if (hw > 0) {
@@ -188,18 +189,60 @@ __global__ void __launch_bounds__(H ? 32 * (H + 1) : 160, 4)
                 named_bar(1, kCtaThreads);
                 const uint32_t nc = s_cmd;
                 if (nc == kCtaStop) break;
+                const uint32_t hint = s_hint;
                 for (uint32_t b = 0; b < nc; b += 32)
                     eval_batch<G, 1, LW, 1>(a, cid, cd, b + (uint32_t)hw * (32 / G), nc, qs, pmin,
                                             pscale, g, r);
-                named_bar(2, kCtaThreads);
+                // The next pop is the first unpopped pool entry or, if one of
+                // this expansion's candidates is accepted below it, that one.
+                // While warp 0 merges, warp 1 reads the pool entry's neighbour
+                // list and asks L2 for their code rows, warp 2 the same for the
+                // nearest candidate. Hints only: the ids are clamped to the
+                // index, and a wrong guess costs L2 traffic, not results.
+                named_bar(2, kCtaThreads);  // every distance is in cd from here
+                uint32_t node = kNoId;
+                if (hw == 1) {
+                    node = hint;
+                } else if (hw == 2 && nc > 0) {
+                    float best = INF;
+                    uint32_t bi = 0;
+                    for (uint32_t c = lane; c < nc; c += 32)
+                        if (cd[c] < best) {
+                            best = cd[c];
+                            bi = c;
+                        }
+#pragma unroll
+                    for (int o = 16; o; o >>= 1) {
+                        const float ob = __shfl_xor_sync(kFull, best, o);
+                        const uint32_t oi = __shfl_xor_sync(kFull, bi, o);
+                        if (ob < best || (ob == best && oi < bi)) {
+                            best = ob;
+                            bi = oi;
+                        }
+                    }
+                    node = cid[bi];
+                }
+                if (node != kNoId) {
+                    node = min(node, a.n - 1u);
+                    const uint32_t* nb = a.nbrs + (size_t)node * a.deg;
+                    for (uint32_t j = lane; j < a.deg; j += 32) {
+                        const uint32_t v = min(__ldg(nb + j), a.n - 1u);
+                        const unsigned char* row = a.codes + (size_t)v * a.cstride;
+                        for (uint32_t off = 0; off < dim; off += 128)
+                            asm volatile("prefetch.global.L2 [%0];" ::"l"(row + off));
+                    }
+                }
             }
             return;
         }
     }
     // distances of cid[0, nc) into cd: this warp alone, or split over the block
-    auto eval_all = [&](uint32_t nc) {
+    auto eval_all = [&](uint32_t nc, uint32_t hint) {
         if constexpr (H > 0) {
-            if (lane == 0) s_cmd = nc;
+            if (lane == 0) {
+                s_cmd = nc;
+                s_hint = hint;
+            }
             __syncwarp();
             named_bar(1, kCtaThreads);
             for (uint32_t b = 0; b < nc; b += 32)
@@ -347,7 +390,7 @@ __global__ void __launch_bounds__(H ? 32 * (H + 1) : 160, 4)
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(a.nbrs + (size_t)(ai[cur] & ~kPopped) *
                                                                          a.deg));
             }
-            eval_all(ncand);
+            eval_all(ncand, cur < alen ? (ai[cur] & ~kPopped) : kNoId);
             calcs += ncand;
             __syncwarp();
 
