@@ -60,22 +60,22 @@ WORKLOADS = {
     "small-100k64": dict(n=100_000, dim=64, gen="uniform", deg=32, efb=200, iters=3,
                          random_edges=4, path_take=64, far_budget=4, nq=1000, k=10,
                          efs=(20, 40, 60, 100, 200), k_extra=100, knn_compare=True),
-    # uneven batch, high dimension (per-query ef and k;
+    # Uneven batch, high dimension (per-query ef and k;
     # CUDA-graph replay timed beside the eager launch)
     "uneven-1m960": dict(n=1_000_000, dim=960, gen="gauss_mixture", clusters=256, sigma=0.3,
                          deg=64, efb=400, iters=3, random_edges=8, path_take=64, far_budget=8,
                          nq=4096, kind="uneven", ef_choices=(32, 64, 128, 256, 512),
                          k_choices=(1, 10, 100)),
-    # index build with BF16 tensor-core pruning against the
+    # Index build with BF16 tensor-core pruning against the
     # FP32 prune (unit-length rows; centre entries N(0, 1), sigma 0.3)
     "build-1m768": dict(n=1_000_000, dim=768, gen="gauss_mixture_unit", clusters=2048, sigma=0.3,
                         deg=64, efb=400, iters=3, random_edges=8, path_take=64, far_budget=8,
                         nq=2000, kind="build", ef=128),
-    # config 4's data at N = 100,000: a build small enough to profile
+    # the build workload's data at N = 100,000: a build small enough to profile
     "build-100k768": dict(n=100_000, dim=768, gen="gauss_mixture_unit", clusters=2048, sigma=0.3,
                           deg=64, efb=400, iters=3, random_edges=8, path_take=64, far_budget=8,
                           nq=2000, kind="build", ef=128),
-    # serving loop, open-loop Poisson arrivals (4 s of
+    # Serving loop, open-loop Poisson arrivals (4 s of
     # arrivals at every rate: 2M distinct queries cover 500 k/s)
     "serving-10m96": dict(n=10_000_000, dim=96, gen="gauss_mixture", clusters=4096, sigma=0.25,
                           deg=32, efb=300, iters=3, random_edges=8, path_take=64, far_budget=8,
@@ -1012,7 +1012,8 @@ def _timed(fn, reps, flush, stream):
 
 
 def uneven_arm(args, w, name, device):
-    """one batch with per-query ef and k, eager and as a CUDA graph."""
+    """The uneven high-dimension batch: one batch with per-query ef and k, eager
+    and as a CUDA graph."""
     import torch
 
     import liteqg_b200
@@ -1242,7 +1243,7 @@ SERVING_STREAMS = 8  # batches in flight at once (each on its own stream)
 
 
 def serving_arm(args, w, name, device):
-    """open-loop Poisson arrivals through the serving loop."""
+    """The serving workload: open-loop Poisson arrivals through the serving loop."""
     import torch
 
     import liteqg_b200
@@ -1359,7 +1360,7 @@ def serving_arm(args, w, name, device):
 
 
 def build_arm(args, w, name, device):
-    """the same data built twice, with the BF16 tensor-core
+    """The build workload: the same data built twice, with the BF16 tensor-core
     prune (pair_kernel 1) and with the FP32 prune (pair_kernel 0); reports the
     build times, the share of pruned edges that differ, recall@10 (best 10 of
     the pool) of the queries at the workload's ef on both indexes, and the
